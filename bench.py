@@ -1,0 +1,359 @@
+"""Benchmark: spin-flip attempts per ns of the B200 parallel-tempering engine.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload maxcut3reg|ea2d] [--impl b200|reference]
+
+Workload (default ``maxcut3reg``): plain PT on MaxCut as Ising over a random 3-regular graph,
+N = 4096 (seeded), J = -1 on edges, h = 0, int8 spins, greedy colouring (4 colours), 64 replicas
+on a geometric beta ladder 0.2..4.0, 1e5 sweeps = 25,000 rounds of 4 sweeps (the reference's
+solve() default sweeps_per_round), one exchange step per round. One "step" is that whole job:
+initialisation plus 1e5 sweeps of all 64 replicas = 2.62e10 attempts.
+
+``value`` is device time (CUDA events around each step, inputs resident in HBM), summed over K
+steps, max over ranks. L2 is flushed (a 256 MiB write) between steps, outside the timed events.
+``e2e`` times the C ABI entry drift_pt_solve with host buffers (layout, upload, run, download).
+With N > 1 (torchrun), every rank runs an independent copy (replicas only: the path has no
+exchange across GPUs) and ``value`` is the sum of all ranks' attempts over the slowest rank's
+time. ``--impl reference`` times the reference's own CPU algorithm (the NumPy restatement of
+drift/solvers/parallel_tempering.py in oracle/ref_pt.py, one process per host core) on a bounded
+sample of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "maxcut3reg": dict(desc="MaxCut random 3-regular N=4096 (J=-1), int8 spins, 64 replicas, beta 0.2-4.0, 1e5 sweeps",
+                       n=4096, seed=2, R=64, beta=(0.2, 4.0), sweeps=100000, spr=4, bytes_per_attempt=2.0 + 3 * 5 / 64),
+    "ea2d": dict(desc="2D EA +-J L=16 periodic (N=256), 24 replicas, beta 0.1-3.0, 2e4 sweeps, swap every sweep",
+                 n=256, seed=1, R=24, beta=(0.1, 3.0), sweeps=20000, spr=1, bytes_per_attempt=2.0 + 4 * 5 / 24),
+}
+
+
+def make_model(name):
+    from drift_b200.instances import ea_2d, maxcut_3regular
+
+    w = WORKLOADS[name]
+    return maxcut_3regular(w["n"], w["seed"]) if name == "maxcut3reg" else ea_2d(16, w["seed"])
+
+
+def ladder(w):
+    b_lo, b_hi = w["beta"]
+    R = w["R"]
+    return b_lo * (b_hi / b_lo) ** (np.arange(R) / (R - 1))
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic(kernel_key):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    return d.get(kernel_key)
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        backend = "nccl" if os.environ.get("DRIFT_BENCH_BACKEND", "nccl") == "nccl" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return rank, world, local
+
+
+def reduce_max(x: float, world: int, device) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------------------------
+
+def run_reference_sample(args_tuple):
+    """One process: the reference CPU algorithm on a bounded sample (1 round x 1 sweep of all rungs)."""
+    name, seed = args_tuple
+    os.environ["OMP_NUM_THREADS"] = "1"
+    sys.path.insert(0, ROOT)
+    from oracle import ref_pt
+
+    w = WORKLOADS[name]
+    model = make_model(name).to_dense()
+    b = ladder(w)
+    t0 = time.perf_counter()
+    out = ref_pt.parallel_tempering(model, n_replicas=w["R"], T_min=1.0 / b[0], T_max=1.0 / b[-1], n_rounds=1,
+                                    sweeps_per_round=1, seed=seed)
+    return out["attempts"], time.perf_counter() - t0
+
+
+def bench_reference(args):
+    rank, world, local = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    import multiprocessing as mp
+
+    w = WORKLOADS[args.workload]
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        for s in range(args.warmup):
+            pool.map(run_reference_sample, [(args.workload, 1000 * s + c) for c in range(cores)])
+        t0 = time.perf_counter()
+        total = 0.0
+        for s in range(args.steps):
+            res = pool.map(run_reference_sample, [(args.workload, 1000 * (s + args.warmup) + c) for c in range(cores)])
+            total += sum(a for a, _ in res)
+        wall = time.perf_counter() - t0
+    v = total / wall / 1e9
+    print(json.dumps({
+        "impl": "reference", "metric": "spin-flips/ns", "value": v, "unit": "flips/ns", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": w["desc"], "sample": f"{cores} processes x (1 round x 1 sweep x {w['R']} rungs x {w['n']} spins) per step"},
+        "cpu_baseline": {"value": v, "unit": "flips/ns", "cores": cores, "kind": "port",
+                         "sample": f"oracle/ref_pt.py (reference CPU PT restated, same NumPy stream), one process per core, "
+                                   f"{cores} x {w['R'] * w['n']:.0f} attempts per step"},
+        "e2e": {"value": v, "unit": "flips/ns", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def cpu_baseline_oracle(w, model_name, budget_s=12.0):
+    """The C oracle (OpenMP over replicas) on the host cores: a bounded number of rounds."""
+    import oracle
+
+    from drift_b200.engine import HostProblem
+
+    hp = HostProblem.from_model(make_model(model_name))
+    prob = oracle.OracleProblem(hp.n, hp.row_ptr, hp.col_idx, hp.weight, hp.h, hp.color_ptr, hp.color_spins)
+    b = ladder(w)
+    threads = os.cpu_count() or 1
+    st = oracle.pt_run(prob, b, n_rounds=1, sweeps_per_round=w["spr"], seed=3, threads=threads)
+    t0 = time.perf_counter()
+    rounds = 0
+    chunk = 2
+    while time.perf_counter() - t0 < budget_s:
+        st = oracle.pt_run(prob, b, n_rounds=chunk, sweeps_per_round=w["spr"], seed=3, threads=threads, state=st,
+                           round_offset=1 + rounds)
+        rounds += chunk
+        chunk = min(chunk * 2, 64)
+    dt = time.perf_counter() - t0
+    attempts = rounds * w["spr"] * w["R"] * w["n"]
+    return {"value": attempts / dt / 1e9, "unit": "flips/ns", "cores": threads, "kind": "port",
+            "sample": f"oracle/pt_oracle.c, {rounds} rounds x {w['spr']} sweeps x {w['R']} replicas x {w['n']} spins "
+                      f"({attempts:.3g} attempts, {dt:.1f} s), OpenMP over replicas"}
+
+
+def bench_b200(args):
+    import ctypes as C
+
+    import torch
+
+    from drift_b200 import _lib
+    from drift_b200.engine import DeviceProblem, HostProblem, PtEngine
+
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    w = WORKLOADS[args.workload]
+    model = make_model(args.workload)
+    hp = HostProblem.from_model(model)
+    prob = DeviceProblem(hp, device=dev)
+    betas = ladder(w)
+    rounds = w["sweeps"] // w["spr"]
+    eng = PtEngine(prob, betas, seed=1, sweeps_per_round=w["spr"], instance=rank)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    attempts_per_step = float(w["R"]) * w["sweeps"] * w["n"]
+
+    def step(seed):
+        eng.seed = seed
+        eng.init()
+        ev_k0.record()
+        eng.run(rounds)
+        ev_k1.record()
+
+    ev_k0, ev_k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for s in range(args.warmup):
+        step(100 + s)
+    eng.check()
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    t_steps, t_kernel = 0.0, 0.0
+    for s in range(args.steps):
+        flush.fill_(s & 0xFF)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step(1000 + s)
+        e1.record()
+        e1.synchronize()
+        t_steps += e0.elapsed_time(e1) * 1e-3
+        t_kernel += ev_k0.elapsed_time(ev_k1) * 1e-3
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    eng.check()
+    t_max = reduce_max(t_steps, world, dev)
+    tk_max = reduce_max(t_kernel, world, dev)
+    value = attempts_per_step * args.steps * world / t_max / 1e9
+
+    # ---- end to end through the C ABI with host buffers ----
+    L = _lib.load()
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    best_s = np.zeros(hp.n, np.float32)
+    bh = np.zeros(rounds)
+    sa = _lib.SolveArgs(w["R"], rounds, w["spr"], 0, 7 + rank, 0.0, 0.0, p(betas))
+    sr = _lib.SolveResult(0, 0, 0, 0, p(best_s), None, None, None, None, p(bh))
+    csr = hp.c_csr()
+    _lib.check(L.drift_pt_solve(C.byref(csr), C.byref(sa), C.byref(sr)), "drift_pt_solve")  # warm
+    e2e_steps = max(1, min(args.steps, 5))
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        _lib.check(L.drift_pt_solve(C.byref(csr), C.byref(sa), C.byref(sr)), "drift_pt_solve")
+    t_e2e = reduce_max(time.perf_counter() - t0, world, dev)
+    e2e = attempts_per_step * e2e_steps * world / t_e2e / 1e9
+    info = prob.info
+    h2d = (hp.n + 1 + prob.info.n_colors + 1 + info.n_slices + 1) * 4 + info.n_ell * 5 + info.n_pos * 4 + w["R"] * 8 \
+        + w["R"] * prob.max_field * 4
+    d2h = w["R"] * 8 * 3 + (w["R"] - 1) * 16 + info.n_pos + rounds * 8
+
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        launch_s = tk_max / args.steps
+        alg_bytes = attempts_per_step * w["bytes_per_attempt"]
+        achieved = alg_bytes / launch_s / 1e9
+        traffic = load_traffic(f"pt_run_kernel/{args.workload}")
+        line = {
+            "metric": "spin-flips/ns", "value": value, "unit": "flips/ns", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int8", "data": "synthetic",
+            "config": {"workload": w["desc"], "rounds": rounds, "sweeps_per_round": w["spr"],
+                       "attempts_per_step": attempts_per_step, "parallelism": f"replicas-only x{world}",
+                       "l2": "flushed between steps (256 MiB write)",
+                       "launch": {"rpc": eng.rpc or "auto", "threads": eng.threads or "auto"}},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "pt_run_kernel", "bytes_per_attempt": w["bytes_per_attempt"],
+                         "kernel_ms": launch_s * 1e3},
+            "e2e": {"value": e2e, "unit": "flips/ns", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "api": "drift_pt_solve (C ABI, host buffers)"},
+            "gpu_launches": 4 * args.steps,
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_oracle(w, args.workload)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="maxcut3reg", choices=list(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        bench_reference(args)
+    else:
+        bench_b200(args)
+
+
+if __name__ == "__main__":
+    main()

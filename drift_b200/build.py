@@ -1,0 +1,58 @@
+"""Build libdrift_pt.so in-tree with nvcc for sm_100a.
+
+    python -m drift_b200.build
+
+The library is loaded by ``drift_b200._lib`` through ctypes. It is built in the package directory
+(not pip-installed, not a JIT cache) so that the built file travels with the source tree.
+"""
+
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIB_PATH = os.path.join(HERE, "libdrift_pt.so")
+ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+SOURCES = ["dpt_host.cpp", "dpt_kernels.cu", "dpt_capi.cu"]
+
+
+def nvcc() -> str:
+    cand = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(cand):
+        raise RuntimeError("nvcc not found: the CUDA toolkit is required to build libdrift_pt.so")
+    return cand
+
+
+def _stale(out: str, deps: list[str]) -> bool:
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    srcs = [os.path.join(CSRC, s) for s in SOURCES]
+    deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    deps.append(os.path.join(os.path.dirname(HERE), "include", "drift_pt.h"))
+    if not force and not _stale(LIB_PATH, deps):
+        return LIB_PATH
+    tmp = LIB_PATH + ".tmp"
+    cmd = [nvcc(), "-O3", "-std=c++17", *ARCH_FLAGS, "-lineinfo", "-shared",
+           "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-Xcompiler", "-fvisibility=hidden",
+           "--expt-relaxed-constexpr", "-o", tmp, *srcs]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed ({r.returncode}):\n{r.stdout}\n{r.stderr}")
+    os.replace(tmp, LIB_PATH)
+    return LIB_PATH
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

@@ -1,0 +1,433 @@
+// dpt_capi.cu - device layer and host convenience entry points of the C ABI (include/drift_pt.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../../include/drift_pt.h"
+#include "dpt_common.cuh"
+#include "dpt_internal.h"
+#include "dpt_kernels.cuh"
+
+using namespace dpt;
+
+namespace {
+
+constexpr size_t kWsHeader = 256;  // barrier counter (u64) at 0, error flag (i32) at 8
+
+struct DeviceInfo {
+  int sm_count = 0;
+  int max_smem_optin = 0;
+};
+
+int device_info(DeviceInfo* di) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return set_error(DRIFT_PT_ECUDA, "cudaGetDevice failed");
+  if (cudaDeviceGetAttribute(&di->sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&di->max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+    return set_error(DRIFT_PT_ECUDA, "cudaDeviceGetAttribute failed");
+  return DRIFT_PT_OK;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return set_error(DRIFT_PT_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+int validate_problem(const DriftPtDeviceProblem* p) {
+  if (!p) return set_error(DRIFT_PT_EINVAL, "problem is NULL");
+  if (p->n < 1 || p->n_pos < p->n || p->n_pos % kSlicePositions || p->n_slices * kSlicePositions != p->n_pos)
+    return set_error(DRIFT_PT_EINVAL, "inconsistent problem sizes (n=%d, n_pos=%d, n_slices=%d)", p->n, p->n_pos, p->n_slices);
+  if (p->n_colors < 1 || p->max_class < 1 || p->n_ell < 0 || p->n_ell % kSlicePositions)
+    return set_error(DRIFT_PT_EINVAL, "inconsistent colouring / ELL sizes");
+  if (!p->color_ptr || !p->slice_off || !p->h_pos || (p->n_ell > 0 && (!p->ell_nbr || !p->ell_w)))
+    return set_error(DRIFT_PT_EINVAL, "problem arrays missing");
+  if (p->integer_path && p->max_field < 1) return set_error(DRIFT_PT_EINVAL, "integer path needs max_field >= 1");
+  return DRIFT_PT_OK;
+}
+
+int validate_state(const DriftPtDeviceState* s, int R) {
+  if (!s || !s->spins || !s->energy || !s->best_energy || !s->best_spins || !s->rung_of_slot || !s->slot_of_rung ||
+      (R > 1 && (!s->swap_tried || !s->swap_accepted)))
+    return set_error(DRIFT_PT_EINVAL, "state arrays missing");
+  return DRIFT_PT_OK;
+}
+
+PtKernelArgs make_args(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, DriftPtDeviceState* s) {
+  PtKernelArgs a;
+  std::memset(&a, 0, sizeof a);
+  a.n = p->n;
+  a.n_pos = p->n_pos;
+  a.n_slices = p->n_slices;
+  a.n_colors = p->n_colors;
+  a.F = p->integer_path ? p->max_field : 0;
+  a.n_ell = p->n_ell;
+  a.color_ptr = p->color_ptr;
+  a.slice_off = p->slice_off;
+  a.ell_nbr = p->ell_nbr;
+  a.ell_w = p->ell_w;
+  a.h_pos = p->h_pos;
+  a.R = r->n_replicas;
+  a.spr = r->sweeps_per_round;
+  a.n_rounds = r->n_rounds;
+  a.round0 = r->round_offset;
+  a.k0 = (uint32_t)(r->seed & 0xffffffffu);
+  a.k1 = (uint32_t)(r->seed >> 32);
+  a.inst = r->instance;
+  a.betas = r->betas;
+  a.thr = r->thresholds;
+  a.spins = s->spins;
+  a.energy = reinterpret_cast<long long*>(s->energy);
+  a.best_energy = reinterpret_cast<long long*>(s->best_energy);
+  a.best_spins = s->best_spins;
+  a.rung_of_slot = s->rung_of_slot;
+  a.slot_of_rung = s->slot_of_rung;
+  a.tried = reinterpret_cast<long long*>(s->swap_tried);
+  a.accepted = reinterpret_cast<long long*>(s->swap_accepted);
+  a.best_hist = s->best_history;
+  return a;
+}
+
+}  // namespace
+
+extern "C" int drift_pt_workspace_bytes(int32_t n_replicas, size_t* bytes) {
+  clear_error();
+  if (n_replicas < 1 || !bytes) return set_error(DRIFT_PT_EINVAL, "workspace_bytes: invalid arguments");
+  *bytes = kWsHeader + ((2 * sizeof(long long) * (size_t)n_replicas + 255) & ~(size_t)255);
+  return DRIFT_PT_OK;
+}
+
+extern "C" int drift_pt_init(const DriftPtDeviceProblem* prob, const DriftPtRunArgs* args,
+                             DriftPtDeviceState* state, void* stream) {
+  clear_error();
+  int rc = validate_problem(prob);
+  if (rc) return rc;
+  if (!args || args->n_replicas < 1) return set_error(DRIFT_PT_EINVAL, "n_replicas must be >= 1");
+  if (args->instance > kMaxInstance) return set_error(DRIFT_PT_EINVAL, "instance must be < 2^24");
+  rc = validate_state(state, args->n_replicas);
+  if (rc) return rc;
+  PtKernelArgs a = make_args(prob, args, state);
+  cudaError_t e = launch_init(a, prob->integer_path, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "drift_pt_init launch");
+  return DRIFT_PT_OK;
+}
+
+namespace {
+
+struct LaunchPlan {
+  int rpc, threads, in_smem, grid;
+  size_t smem;
+};
+
+int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPlan* lp) {
+  DeviceInfo di;
+  int rc = device_info(&di);
+  if (rc) return rc;
+  const int R = r->n_replicas;
+  const int ip = p->integer_path;
+  auto total = [&](int rpc, bool ell) {
+    return smem_layout(p->n_pos, rpc, R, p->max_field, p->n_colors, p->n_slices, p->n_ell, ip != 0, ell).total;
+  };
+  int rpc = r->replicas_per_cta;
+  if (rpc <= 0) {
+    // Work of one round on one replica vs the cost of a grid-wide barrier (~1-2 us): small
+    // problems keep every replica in one CTA and need no barrier at all.
+    const double work = (double)R * p->n * std::max(1, r->sweeps_per_round);
+    if (work <= 65536.0 && total(R, false) <= (size_t)di.max_smem_optin) rpc = R;
+    else rpc = 1;
+  }
+  rpc = std::min(rpc, R);
+  while (rpc < R && (R + rpc - 1) / rpc > di.sm_count) rpc *= 2;
+  rpc = std::min(rpc, R);
+  if (total(rpc, false) > (size_t)di.max_smem_optin)
+    return set_error(DRIFT_PT_EUNSUPPORTED, "replica state of %d x %d positions exceeds shared memory (%d B)", rpc,
+                     p->n_pos, di.max_smem_optin);
+  const bool in_smem = total(rpc, true) <= (size_t)di.max_smem_optin;
+  int threads = r->threads_per_cta;
+  if (threads <= 0) {
+    const int groups = p->max_class / kGroup + 2;
+    threads = std::min(1024, std::max(64, ((rpc * groups + 31) / 32) * 32));
+  }
+  if (threads < 32 || threads > 1024 || threads % 32) return set_error(DRIFT_PT_EINVAL, "threads_per_cta must be a multiple of 32 in [32, 1024]");
+  lp->rpc = rpc;
+  lp->threads = threads;
+  lp->in_smem = in_smem ? 1 : 0;
+  lp->grid = (R + rpc - 1) / rpc;
+  lp->smem = total(rpc, in_smem);
+  const void* fn = run_kernel_ptr(ip, lp->in_smem);
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lp->smem);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, lp->smem);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+  if ((long long)per_sm * di.sm_count < lp->grid)
+    return set_error(DRIFT_PT_EUNSUPPORTED, "%d CTAs of %d threads / %zu B shared memory cannot be co-resident (%d per SM x %d SMs)",
+                     lp->grid, threads, lp->smem, per_sm, di.sm_count);
+  return DRIFT_PT_OK;
+}
+
+}  // namespace
+
+extern "C" int drift_pt_run(const DriftPtDeviceProblem* prob, const DriftPtRunArgs* args,
+                            DriftPtDeviceState* state, void* workspace, size_t workspace_bytes, void* stream) {
+  clear_error();
+  int rc = validate_problem(prob);
+  if (rc) return rc;
+  if (!args || args->n_replicas < 1 || args->n_rounds < 0 || args->sweeps_per_round < 1 || args->round_offset < 0)
+    return set_error(DRIFT_PT_EINVAL, "run args: need n_replicas >= 1, n_rounds >= 0, sweeps_per_round >= 1");
+  if (args->instance > kMaxInstance) return set_error(DRIFT_PT_EINVAL, "instance must be < 2^24");
+  if (!args->betas || (prob->integer_path && !args->thresholds))
+    return set_error(DRIFT_PT_EINVAL, "run args: betas (and thresholds on the integer path) are required");
+  rc = validate_state(state, args->n_replicas);
+  if (rc) return rc;
+  size_t need = 0;
+  drift_pt_workspace_bytes(args->n_replicas, &need);
+  if (!workspace || workspace_bytes < need)
+    return set_error(DRIFT_PT_EINVAL, "workspace of %zu bytes is smaller than the %zu required", workspace_bytes, need);
+  if (args->n_rounds == 0) return DRIFT_PT_OK;
+  LaunchPlan lp;
+  rc = plan_launch(prob, args, &lp);
+  if (rc) return rc;
+  PtKernelArgs a = make_args(prob, args, state);
+  a.rpc = lp.rpc;
+  unsigned char* ws = static_cast<unsigned char*>(workspace);
+  a.bar = reinterpret_cast<unsigned long long*>(ws);
+  a.err = reinterpret_cast<int*>(ws + 8);
+  a.pub = reinterpret_cast<long long*>(ws + kWsHeader);
+  const double to = args->timeout_s > 0 ? args->timeout_s : 10.0;
+  a.timeout_ns = (long long)(to * 1e9);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemsetAsync(ws, 0, kWsHeader, st);
+  if (e != cudaSuccess) return cuda_fail(e, "workspace reset");
+  cudaLaunchConfig_t cfg;
+  std::memset(&cfg, 0, sizeof cfg);
+  cfg.gridDim = dim3(lp.grid);
+  cfg.blockDim = dim3(lp.threads);
+  cfg.dynamicSmemBytes = lp.smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  void* kargs[] = {&a};
+  e = cudaLaunchKernelExC(&cfg, run_kernel_ptr(prob->integer_path, lp.in_smem), kargs);
+  if (e != cudaSuccess) return cuda_fail(e, "pt_run_kernel launch");
+  return DRIFT_PT_OK;
+}
+
+extern "C" int drift_pt_check(void* workspace, void* stream) {
+  clear_error();
+  if (!workspace) return set_error(DRIFT_PT_EINVAL, "workspace is NULL");
+  cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "stream synchronize");
+  int flag = 0;
+  e = cudaMemcpy(&flag, static_cast<unsigned char*>(workspace) + 8, sizeof flag, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "error flag read");
+  if (flag) return set_error(DRIFT_PT_ETIMEOUT, "a bounded in-kernel wait timed out (flag %d); the state is incomplete", flag);
+  return DRIFT_PT_OK;
+}
+
+extern "C" int drift_pt_energy_fp64(const DriftPtDeviceProblem* prob, const int8_t* spins, int32_t n_replicas,
+                                    double* out, void* stream) {
+  clear_error();
+  int rc = validate_problem(prob);
+  if (rc) return rc;
+  if (!spins || !out || n_replicas < 1) return set_error(DRIFT_PT_EINVAL, "energy_fp64: invalid arguments");
+  DriftPtRunArgs r;
+  std::memset(&r, 0, sizeof r);
+  r.n_replicas = n_replicas;
+  DriftPtDeviceState s;
+  std::memset(&s, 0, sizeof s);
+  PtKernelArgs a = make_args(prob, &r, &s);
+  cudaError_t e = launch_energy_fp64(a, prob->integer_path, spins, n_replicas, out, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "energy_fp64 launch");
+  return DRIFT_PT_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// drift_pt_solve: host buffers in, host results out.
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+struct DeviceArena {
+  void* base = nullptr;
+  ~DeviceArena() {
+    if (base) cudaFree(base);
+  }
+};
+
+size_t bump(size_t& off, size_t bytes) {
+  size_t o = off;
+  off = (off + bytes + 255) & ~(size_t)255;
+  return o;
+}
+
+}  // namespace
+
+extern "C" int drift_pt_solve(const DriftPtCsr* csr, const DriftPtSolveArgs* args, DriftPtSolveResult* out) {
+  clear_error();
+  if (!args || !out || !out->best_s) return set_error(DRIFT_PT_EINVAL, "solve: args/out/best_s required");
+  const int R = args->n_replicas;
+  if (R < 1 || args->n_rounds < 0 || args->sweeps_per_round < 1)
+    return set_error(DRIFT_PT_EINVAL, "solve: need n_replicas >= 1, n_rounds >= 0, sweeps_per_round >= 1");
+  DriftPtLayoutInfo info;
+  int rc = drift_pt_layout_query(csr, &info);
+  if (rc) return rc;
+  const int ip = info.integer_couplings;
+  // ---- ladder (drift/solvers/parallel_tempering.py:29-36,72-73) ----
+  std::vector<double> betas((size_t)R);
+  if (args->betas) {
+    for (int r = 0; r < R; ++r) betas[r] = args->betas[r];
+  } else {
+    if (!(args->T_min > 0.0) || !(args->T_max > 0.0)) return set_error(DRIFT_PT_EINVAL, "solve: T_min and T_max must be > 0");
+    for (int r = 0; r < R; ++r) {
+      double T = (R == 1) ? args->T_min : args->T_min * std::pow(args->T_max / args->T_min, (double)r / (R - 1));
+      betas[r] = 1.0 / std::max(T, 1e-12);
+    }
+  }
+  std::vector<uint32_t> thr;
+  if (ip) {
+    thr.resize((size_t)R * info.max_field);
+    rc = drift_pt_thresholds(R, betas.data(), info.max_field, thr.data());
+    if (rc) return rc;
+  }
+  // ---- host layout ----
+  std::vector<int32_t> color_ptr(info.n_colors + 1), slice_off(info.n_slices + 1), ell_nbr(info.n_ell),
+      site_of_pos(info.n_pos), pos_of_site(info.n);
+  std::vector<unsigned char> ell_w((size_t)info.n_ell * (ip ? 1 : 4)), h_pos((size_t)info.n_pos * 4);
+  DriftPtLayout lay{color_ptr.data(), slice_off.data(), ell_nbr.data(), ell_w.data(), h_pos.data(), site_of_pos.data(),
+                    pos_of_site.data()};
+  rc = drift_pt_layout_fill(csr, ip, &lay);
+  if (rc) return rc;
+  int max_class = 1;
+  for (int c = 0; c < info.n_colors; ++c) max_class = std::max(max_class, color_ptr[c + 1] - color_ptr[c]);
+  // ---- device arena ----
+  size_t ws_bytes = 0;
+  drift_pt_workspace_bytes(R, &ws_bytes);
+  size_t off = 0;
+  const size_t o_cp = bump(off, color_ptr.size() * 4), o_so = bump(off, slice_off.size() * 4),
+               o_nb = bump(off, ell_nbr.size() * 4), o_w = bump(off, ell_w.size()), o_h = bump(off, h_pos.size()),
+               o_beta = bump(off, (size_t)R * 8), o_thr = bump(off, thr.size() * 4),
+               o_sp = bump(off, (size_t)R * info.n_pos), o_bsp = bump(off, (size_t)R * info.n_pos),
+               o_e = bump(off, (size_t)R * 8), o_be = bump(off, (size_t)R * 8), o_rs = bump(off, (size_t)R * 4),
+               o_sr = bump(off, (size_t)R * 4), o_tr = bump(off, (size_t)R * 8), o_ac = bump(off, (size_t)R * 8),
+               o_bh = bump(off, (size_t)std::max(1, args->n_rounds) * 8), o_ws = bump(off, ws_bytes);
+  DeviceArena arena;
+  cudaError_t e = cudaMalloc(&arena.base, off);
+  if (e != cudaSuccess) {
+    arena.base = nullptr;
+    return set_error(DRIFT_PT_ENOMEM, "cudaMalloc of %zu bytes failed: %s", off, cudaGetErrorString(e));
+  }
+  unsigned char* d = static_cast<unsigned char*>(arena.base);
+  auto h2d = [&](size_t o, const void* src, size_t bytes) -> cudaError_t {
+    return bytes ? cudaMemcpy(d + o, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
+  };
+  if ((e = h2d(o_cp, color_ptr.data(), color_ptr.size() * 4)) != cudaSuccess ||
+      (e = h2d(o_so, slice_off.data(), slice_off.size() * 4)) != cudaSuccess ||
+      (e = h2d(o_nb, ell_nbr.data(), ell_nbr.size() * 4)) != cudaSuccess ||
+      (e = h2d(o_w, ell_w.data(), ell_w.size())) != cudaSuccess || (e = h2d(o_h, h_pos.data(), h_pos.size())) != cudaSuccess ||
+      (e = h2d(o_beta, betas.data(), (size_t)R * 8)) != cudaSuccess || (e = h2d(o_thr, thr.data(), thr.size() * 4)) != cudaSuccess)
+    return cuda_fail(e, "solve: upload");
+  DriftPtDeviceProblem prob;
+  std::memset(&prob, 0, sizeof prob);
+  prob.n = info.n;
+  prob.n_pos = info.n_pos;
+  prob.n_slices = info.n_slices;
+  prob.n_colors = info.n_colors;
+  prob.integer_path = ip;
+  prob.max_field = info.max_field;
+  prob.max_width = info.max_degree;
+  prob.max_class = max_class;
+  prob.n_ell = info.n_ell;
+  prob.color_ptr = reinterpret_cast<const int32_t*>(d + o_cp);
+  prob.slice_off = reinterpret_cast<const int32_t*>(d + o_so);
+  prob.ell_nbr = reinterpret_cast<const int32_t*>(d + o_nb);
+  prob.ell_w = d + o_w;
+  prob.h_pos = d + o_h;
+  DriftPtDeviceState st;
+  st.spins = reinterpret_cast<int8_t*>(d + o_sp);
+  st.best_spins = reinterpret_cast<int8_t*>(d + o_bsp);
+  st.energy = reinterpret_cast<int64_t*>(d + o_e);
+  st.best_energy = reinterpret_cast<int64_t*>(d + o_be);
+  st.rung_of_slot = reinterpret_cast<int32_t*>(d + o_rs);
+  st.slot_of_rung = reinterpret_cast<int32_t*>(d + o_sr);
+  st.swap_tried = reinterpret_cast<int64_t*>(d + o_tr);
+  st.swap_accepted = reinterpret_cast<int64_t*>(d + o_ac);
+  st.best_history = reinterpret_cast<double*>(d + o_bh);
+  DriftPtRunArgs ra;
+  std::memset(&ra, 0, sizeof ra);
+  ra.n_replicas = R;
+  ra.n_rounds = args->n_rounds;
+  ra.sweeps_per_round = args->sweeps_per_round;
+  ra.seed = args->seed;
+  ra.betas = reinterpret_cast<const double*>(d + o_beta);
+  ra.thresholds = ip ? reinterpret_cast<const uint32_t*>(d + o_thr) : nullptr;
+  rc = drift_pt_init(&prob, &ra, &st, nullptr);
+  if (rc) return rc;
+  cudaEvent_t ev0, ev1;
+  cudaEventCreate(&ev0);
+  cudaEventCreate(&ev1);
+  cudaEventRecord(ev0, nullptr);
+  rc = drift_pt_run(&prob, &ra, &st, d + o_ws, ws_bytes, nullptr);
+  cudaEventRecord(ev1, nullptr);
+  if (rc == DRIFT_PT_OK) rc = drift_pt_check(d + o_ws, nullptr);
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, ev0, ev1);
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  if (rc) return rc;
+  // ---- results ----
+  std::vector<long long> be(R), en(R);
+  std::vector<int32_t> slot_of_rung(R);
+  std::vector<long long> tried(std::max(1, R - 1)), acc(std::max(1, R - 1));
+  if ((e = cudaMemcpy(be.data(), d + o_be, (size_t)R * 8, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+      (e = cudaMemcpy(en.data(), d + o_e, (size_t)R * 8, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+      (e = cudaMemcpy(slot_of_rung.data(), d + o_sr, (size_t)R * 4, cudaMemcpyDeviceToHost)) != cudaSuccess)
+    return cuda_fail(e, "solve: download");
+  if (R > 1 && ((e = cudaMemcpy(tried.data(), d + o_tr, (size_t)(R - 1) * 8, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+                (e = cudaMemcpy(acc.data(), d + o_ac, (size_t)(R - 1) * 8, cudaMemcpyDeviceToHost)) != cudaSuccess))
+    return cuda_fail(e, "solve: download stats");
+  int best = 0;
+  for (int r = 1; r < R; ++r)
+    if (be[r] < be[best]) best = r;
+  std::vector<int8_t> bs(info.n_pos);
+  if ((e = cudaMemcpy(bs.data(), d + o_bsp + (size_t)best * info.n_pos, info.n_pos, cudaMemcpyDeviceToHost)) != cudaSuccess)
+    return cuda_fail(e, "solve: download best");
+  for (int p = 0; p < info.n; ++p) out->best_s[site_of_pos[p]] = (float)bs[p];
+  // best_E in FP64 from the configuration itself (E = -1/2 s.J.s - h.s, drift/ising.py:50-53)
+  double E = 0.0;
+  for (int i = 0; i < info.n; ++i) {
+    double f = 0.0;
+    for (int t = csr->row_ptr[i]; t < csr->row_ptr[i + 1]; ++t) f += (double)csr->weight[t] * out->best_s[csr->col_idx[t]];
+    E += -0.5 * out->best_s[i] * f - (double)csr->h[i] * out->best_s[i];
+  }
+  out->best_E = E;
+  out->seconds = ms * 1e-3;
+  out->throughput = out->seconds > 0 ? (double)R * args->n_rounds * args->sweeps_per_round * info.n / out->seconds : 0.0;
+  long long tt = 0, ta = 0;
+  for (int r = 0; r + 1 < R; ++r) {
+    tt += tried[r];
+    ta += acc[r];
+  }
+  out->swap_rate = tt ? (double)ta / (double)tt : 0.0;
+  if (out->swap_tried)
+    for (int r = 0; r + 1 < R; ++r) out->swap_tried[r] = tried[r];
+  if (out->swap_accepted)
+    for (int r = 0; r + 1 < R; ++r) out->swap_accepted[r] = acc[r];
+  if (out->rung_energy)
+    for (int r = 0; r < R; ++r) out->rung_energy[r] = ip ? (double)en[slot_of_rung[r]] : (double)en[slot_of_rung[r]] * kFloatEnergyScale;
+  if (out->rung_spins) {
+    std::vector<int8_t> sp((size_t)R * info.n_pos);
+    if ((e = cudaMemcpy(sp.data(), d + o_sp, sp.size(), cudaMemcpyDeviceToHost)) != cudaSuccess)
+      return cuda_fail(e, "solve: download spins");
+    for (int r = 0; r < R; ++r)
+      for (int p = 0; p < info.n; ++p)
+        out->rung_spins[(size_t)r * info.n + site_of_pos[p]] = sp[(size_t)slot_of_rung[r] * info.n_pos + p];
+  }
+  if (out->best_history && args->n_rounds > 0)
+    if ((e = cudaMemcpy(out->best_history, d + o_bh, (size_t)args->n_rounds * 8, cudaMemcpyDeviceToHost)) != cudaSuccess)
+      return cuda_fail(e, "solve: download history");
+  return DRIFT_PT_OK;
+}

@@ -1,0 +1,16 @@
+// dpt_internal.h - declarations shared by the translation units of libdrift_pt (not public ABI).
+#pragma once
+#include <cstdarg>
+#include <cstdint>
+
+namespace dpt {
+
+// Sliced-ELL geometry: a thread owns a group of 8 consecutive positions, a warp 32 groups,
+// so one slice of the coupling table covers 256 positions.
+constexpr int kGroup = 8;
+constexpr int kSlicePositions = 256;
+
+int set_error(int code, const char* fmt, ...);
+void clear_error();
+
+}  // namespace dpt

@@ -1,0 +1,490 @@
+// dpt_kernels.cu - sm_100a kernels of the parallel-tempering engine.
+//
+// One persistent cooperative launch runs every round of a PT job (the reference launches a sweep
+// kernel and a swap kernel per round from a host loop, cuda/ising_pt.cu:214-218):
+//   * each CTA owns `rpc` replica slots; their int8 spins live in shared memory for the whole
+//     launch, together with the coupling table when it fits (otherwise it is read through L1/L2);
+//   * a sweep is one phase per colour class; within a phase every (slot, group of 8 consecutive
+//     positions) item is independent, so threads take items in any order and results do not
+//     depend on the launch shape;
+//   * Metropolis acceptance uses counter-based Philox uniforms and, on the integer path, a
+//     per-rung threshold table (no exp in the loop); energies are updated incrementally in exact
+//     fixed point;
+//   * after each round every CTA publishes its slots' energies, meets the others at a bounded
+//     grid barrier, and all CTAs evaluate the same adjacent-rung exchange step redundantly.
+#include <climits>
+#include <cuda_runtime.h>
+
+#include "../../include/drift_pt.h"
+#include "dpt_common.cuh"
+#include "dpt_internal.h"
+#include "dpt_kernels.cuh"
+
+namespace dpt {
+
+__device__ __forceinline__ unsigned long long global_timer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ int ld_relaxed_i32(const int* p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+template <bool kInSmem, typename T>
+__device__ __forceinline__ T ld_table(const T* p) {
+  if constexpr (kInSmem) return *p;
+  else return __ldg(p);
+}
+
+// ---------------------------------------------------------------------------------------------
+// One item: positions 8g .. 8g+7 of one replica slot, restricted to colour range [lo, hi).
+// ---------------------------------------------------------------------------------------------
+template <bool kInt, bool kInSmem>
+__device__ __forceinline__ long long sweep_group(int g, int lo, int hi, uint32_t t, int slot,
+                                                 int8_t* __restrict__ sp,
+                                                 const int* __restrict__ soff,
+                                                 const int* __restrict__ nbr,
+                                                 const void* __restrict__ wv,
+                                                 const void* __restrict__ hv,
+                                                 const uint32_t* __restrict__ thr_rung, int F,
+                                                 float neg2beta, uint32_t inst, uint32_t k0,
+                                                 uint32_t k1) {
+  const U4 rnd = philox(U4{(uint32_t)g, t, (uint32_t)slot, ctr3(kTagSweep, inst)}, k0, k1);
+  const uint32_t words[4] = {rnd.x, rnd.y, rnd.z, rnd.w};
+  uint64_t s8 = *reinterpret_cast<const uint64_t*>(sp + (size_t)g * kGroup);
+  const int S = g >> 5, lane = g & 31;
+  const int w0 = ld_table<kInSmem>(soff + S), w1 = ld_table<kInSmem>(soff + S + 1);
+  const int width = w1 - w0;
+  const long long base = (long long)w0 * kSlicePositions + lane;
+  const long long hbase = (long long)S * kSlicePositions + lane;
+  long long dacc = 0;
+#pragma unroll
+  for (int q = 0; q < kGroup; ++q) {
+    const int p = g * kGroup + q;
+    if (p < lo || p >= hi) continue;
+    const int si = (int)(int8_t)(uint8_t)(s8 >> (8 * q));
+    bool acc;
+    uint32_t thr = 0;
+    long long dE = 0;
+    if constexpr (kInt) {
+      const int8_t* w = static_cast<const int8_t*>(wv);
+      int field = ld_table<kInSmem>(static_cast<const int*>(hv) + hbase + q * 32);
+      for (int d = 0; d < width; ++d) {
+        const long long e = base + (long long)(d * kGroup + q) * 32;
+        field += (int)ld_table<kInSmem>(w + e) * (int)sp[ld_table<kInSmem>(nbr + e)];
+      }
+      int x = si * field;
+      acc = (x <= 0);
+      if (!acc) thr = thr_rung[min(x, F) - 1];
+      dE = 2LL * x;
+    } else {
+      const float* w = static_cast<const float*>(wv);
+      float field = ld_table<kInSmem>(static_cast<const float*>(hv) + hbase + q * 32);
+      for (int d = 0; d < width; ++d) {
+        const long long e = base + (long long)(d * kGroup + q) * 32;
+        const float wt = ld_table<kInSmem>(w + e);
+        field = f_add(field, sp[ld_table<kInSmem>(nbr + e)] > 0 ? wt : -wt);
+      }
+      const float x = si > 0 ? field : -field;
+      acc = !(x > 0.0f);
+      if (!acc) thr = threshold_f(neg2beta, x);
+      dE = f_to_ll_rn(f_mul(x, 2.0f * kFloatEnergyQuant));
+    }
+    if (!acc) {
+      const uint32_t prim = (words[q >> 1] >> ((q & 1) * 16)) & 0xFFFFu;
+      const uint32_t th = thr >> 16;
+      acc = prim < th;
+      if (prim == th) {  // the first 16 bits tie: draw the second half of this uniform
+        const U4 r2 = philox(U4{(uint32_t)p, t, (uint32_t)slot, ctr3(kTagSecond, inst)}, k0, k1);
+        acc = (r2.x & 0xFFFFu) < (thr & 0xFFFFu);
+      }
+    }
+    if (acc) {
+      s8 ^= (uint64_t)0xFEu << (8 * q);  // +1 (0x01) <-> -1 (0xFF)
+      dacc += dE;
+    }
+  }
+  *reinterpret_cast<uint64_t*>(sp + (size_t)g * kGroup) = s8;
+  return dacc;
+}
+
+template <bool kInt, bool kInSmem>
+__global__ void __launch_bounds__(1024, 1) pt_run_kernel(const PtKernelArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const SmemLayout L = smem_layout(a.n_pos, a.rpc, a.R, a.F, a.n_colors, a.n_slices, a.n_ell, kInt, kInSmem);
+  int8_t* sp = reinterpret_cast<int8_t*>(smem + L.spins);
+  long long* eacc = reinterpret_cast<long long*>(smem + L.eacc);
+  long long* ecur = reinterpret_cast<long long*>(smem + L.ecur);
+  long long* ebest = reinterpret_cast<long long*>(smem + L.ebest);
+  int* imp = reinterpret_cast<int*>(smem + L.imp);
+  long long* eall = reinterpret_cast<long long*>(smem + L.eall);
+  int* rung_sm = reinterpret_cast<int*>(smem + L.rung);
+  int* slot_sm = reinterpret_cast<int*>(smem + L.slot);
+  double* beta_sm = reinterpret_cast<double*>(smem + L.beta);
+  float* nb_sm = reinterpret_cast<float*>(smem + L.nb);
+  uint32_t* thr_sm = reinterpret_cast<uint32_t*>(smem + L.thr);
+  int* stats = reinterpret_cast<int*>(smem + L.stats);
+  int* cptr = reinterpret_cast<int*>(smem + L.cptr);
+  int* ctl = reinterpret_cast<int*>(smem + L.ctl);
+
+  const int tid = threadIdx.x, B = blockDim.x;
+  const int R = a.R, n_pos = a.n_pos;
+  const int s0 = blockIdx.x * a.rpc;
+  const int nloc = min(a.rpc, R - s0);
+
+  // ---- stage state and tables ----
+  {
+    const int4* src = reinterpret_cast<const int4*>(a.spins + (size_t)s0 * n_pos);
+    int4* dst = reinterpret_cast<int4*>(sp);
+    const int nv = nloc * n_pos / 16;
+    for (int i = tid; i < nv; i += B) dst[i] = src[i];
+  }
+  for (int i = tid; i < nloc; i += B) {
+    eacc[i] = 0;
+    ecur[i] = a.energy[s0 + i];
+    ebest[i] = a.best_energy[s0 + i];
+    imp[i] = 0;
+  }
+  for (int i = tid; i < R; i += B) {
+    rung_sm[i] = a.rung_of_slot[i];
+    slot_sm[i] = a.slot_of_rung[i];
+    beta_sm[i] = a.betas[i];
+  }
+  if constexpr (kInt)
+    for (int i = tid; i < R * a.F; i += B) thr_sm[i] = a.thr[i];
+  for (int i = tid; i < 2 * (R - 1); i += B) stats[i] = 0;
+  for (int i = tid; i <= a.n_colors; i += B) cptr[i] = a.color_ptr[i];
+  const int* soff = a.slice_off;
+  const int* nbr = a.ell_nbr;
+  const void* wv = a.ell_w;
+  const void* hv = a.h_pos;
+  if constexpr (kInSmem) {
+    int* soff_sm = reinterpret_cast<int*>(smem + L.soff);
+    int* nbr_sm = reinterpret_cast<int*>(smem + L.nbr);
+    for (int i = tid; i <= a.n_slices; i += B) soff_sm[i] = a.slice_off[i];
+    {
+      const int4* s4 = reinterpret_cast<const int4*>(a.ell_nbr);
+      int4* d4 = reinterpret_cast<int4*>(nbr_sm);
+      for (long long i = tid; i < a.n_ell / 4; i += B) d4[i] = s4[i];
+    }
+    {
+      const long long wbytes = kInt ? a.n_ell : a.n_ell * 4;
+      const int4* s4 = reinterpret_cast<const int4*>(a.ell_w);
+      int4* d4 = reinterpret_cast<int4*>(smem + L.w);
+      for (long long i = tid; i < wbytes / 16; i += B) d4[i] = s4[i];
+    }
+    {
+      const int4* s4 = reinterpret_cast<const int4*>(a.h_pos);
+      int4* d4 = reinterpret_cast<int4*>(smem + L.h);
+      for (int i = tid; i < n_pos / 4; i += B) d4[i] = s4[i];
+    }
+    soff = soff_sm;
+    nbr = nbr_sm;
+    wv = smem + L.w;
+    hv = smem + L.h;
+  }
+  if (tid == 0) {
+    ctl[0] = 0;  // abort flag
+    long long b = a.best_energy[0];
+    for (int i = 1; i < R; ++i) b = min(b, a.best_energy[i]);
+    reinterpret_cast<long long*>(ctl + 2)[0] = b;  // running best (CTA 0 uses it)
+  }
+  __syncthreads();
+  if constexpr (!kInt)
+    for (int i = tid; i < nloc; i += B) nb_sm[i] = -2.0f * (float)beta_sm[rung_sm[s0 + i]];
+  __syncthreads();
+
+  const int k = a.n_colors;
+  for (int j = 0; j < a.n_rounds; ++j) {
+    const long long round = a.round0 + j;
+    for (int sw = 0; sw < a.spr; ++sw) {
+      const uint32_t t = (uint32_t)(round * a.spr + sw);
+      for (int c = 0; c < k; ++c) {
+        const int lo = cptr[c], hi = cptr[c + 1];
+        const int glo = lo >> 3, ghi = (hi + 7) >> 3, ng = ghi - glo;
+        const int items = nloc * ng;
+        for (int it = tid; it < items; it += B) {
+          const int sl = (nloc == 1) ? 0 : it / ng;
+          const int g = glo + (it - sl * ng);
+          const int slot = s0 + sl;
+          const long long d = sweep_group<kInt, kInSmem>(
+              g, lo, hi, t, slot, sp + (size_t)sl * n_pos, soff, nbr, wv, hv,
+              kInt ? thr_sm + (size_t)rung_sm[slot] * a.F : nullptr, a.F,
+              kInt ? 0.0f : nb_sm[sl], a.inst, a.k0, a.k1);
+          if (d != 0) atomicAdd(reinterpret_cast<unsigned long long*>(eacc + sl), (unsigned long long)d);
+        }
+        __syncthreads();
+      }
+    }
+    // ---- round end: energies, per-slot best, publication ----
+    for (int i = tid; i < nloc; i += B) {
+      const long long e = ecur[i] + eacc[i];
+      eacc[i] = 0;
+      ecur[i] = e;
+      imp[i] = (e < ebest[i]) ? 1 : 0;
+      if (e < ebest[i]) ebest[i] = e;
+      if (gridDim.x > 1) __stcg(a.pub + (size_t)(round & 1) * R + s0 + i, e);
+    }
+    __syncthreads();
+    for (int sl = 0; sl < nloc; ++sl) {
+      if (!imp[sl]) continue;  // uniform across the block
+      const int4* src = reinterpret_cast<const int4*>(sp + (size_t)sl * n_pos);
+      int4* dst = reinterpret_cast<int4*>(a.best_spins + (size_t)(s0 + sl) * n_pos);
+      for (int i = tid; i < n_pos / 16; i += B) dst[i] = src[i];
+    }
+    if (gridDim.x > 1) {
+      if (tid == 0) {
+        __threadfence();
+        atomicAdd(a.bar, 1ULL);
+        const unsigned long long target = (unsigned long long)(j + 1) * gridDim.x;
+        const unsigned long long t0 = global_timer_ns();
+        int abort_now = 0;
+        while (ld_acquire_u64(a.bar) < target) {
+          if (ld_relaxed_i32(a.err) != 0) { abort_now = 1; break; }
+          if (global_timer_ns() - t0 > (unsigned long long)a.timeout_ns) {
+            atomicExch(a.err, DRIFT_PT_ETIMEOUT);
+            abort_now = 1;
+            break;
+          }
+        }
+        ctl[0] = abort_now;
+      }
+      __syncthreads();
+      if (ctl[0]) break;
+      for (int i = tid; i < R; i += B) eall[i] = __ldcg(a.pub + (size_t)(round & 1) * R + i);
+    } else {
+      for (int i = tid; i < R; i += B) eall[i] = ecur[i];
+    }
+    __syncthreads();
+    // ---- exchange step: identical in every CTA (disjoint pairs, one lane per pair) ----
+    if (tid < 32) {
+      const int parity = (int)(round & 1);
+      for (int r = parity + 2 * tid; r + 1 < R; r += 64) {
+        const int sa = slot_sm[r], sb = slot_sm[r + 1];
+        const long long de = eall[sa] - eall[sb];
+        const double ded = kInt ? (double)de : d_mul((double)de, kFloatEnergyScale);
+        const double delta = d_mul(d_sub(beta_sm[r], beta_sm[r + 1]), ded);
+        bool acc = delta >= 0.0;
+        if (!acc) {
+          const U4 u = philox(U4{(uint32_t)r, (uint32_t)round, (uint32_t)((unsigned long long)round >> 32),
+                                 ctr3(kTagSwap, a.inst)}, a.k0, a.k1);
+          acc = uniform53(u.x, u.y) < exp_neg_d(delta);
+        }
+        if (blockIdx.x == 0) {
+          stats[2 * r] += 1;
+          stats[2 * r + 1] += acc ? 1 : 0;
+        }
+        if (acc) {
+          slot_sm[r] = sb;
+          slot_sm[r + 1] = sa;
+          rung_sm[sa] = r + 1;
+          rung_sm[sb] = r;
+        }
+      }
+      if (blockIdx.x == 0 && a.best_hist) {
+        long long m = LLONG_MAX;
+        for (int i = tid; i < R; i += 32) m = min(m, eall[i]);
+        for (int off = 16; off > 0; off >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, off));
+        if (tid == 0) {
+          long long* rb = reinterpret_cast<long long*>(ctl + 2);
+          rb[0] = min(rb[0], m);
+          a.best_hist[j] = kInt ? (double)rb[0] : d_mul((double)rb[0], kFloatEnergyScale);
+        }
+      }
+    }
+    __syncthreads();
+    if constexpr (!kInt) {
+      for (int i = tid; i < nloc; i += B) nb_sm[i] = -2.0f * (float)beta_sm[rung_sm[s0 + i]];
+      __syncthreads();
+    }
+  }
+
+  // ---- write back ----
+  __syncthreads();
+  {
+    const int4* src = reinterpret_cast<const int4*>(sp);
+    int4* dst = reinterpret_cast<int4*>(a.spins + (size_t)s0 * n_pos);
+    const int nv = nloc * n_pos / 16;
+    for (int i = tid; i < nv; i += B) dst[i] = src[i];
+  }
+  for (int i = tid; i < nloc; i += B) {
+    a.energy[s0 + i] = ecur[i];
+    a.best_energy[s0 + i] = ebest[i];
+  }
+  if (blockIdx.x == 0) {
+    for (int i = tid; i < R; i += B) {
+      a.rung_of_slot[i] = rung_sm[i];
+      a.slot_of_rung[i] = slot_sm[i];
+    }
+    for (int r = tid; r < R - 1; r += B) {
+      a.tried[r] += stats[2 * r];
+      a.accepted[r] += stats[2 * r + 1];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Initialisation
+// ---------------------------------------------------------------------------------------------
+__global__ void init_spins_kernel(int n, int n_pos, int R, uint32_t inst, uint32_t k0, uint32_t k1,
+                                  int8_t* spins, int8_t* best_spins) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int slot = blockIdx.y;
+  if (g * kGroup >= n_pos || slot >= R) return;
+  uint64_t s8 = 0;
+#pragma unroll
+  for (int half = 0; half < 2; ++half) {
+    const int p0 = g * kGroup + half * 4;
+    const U4 u = philox(U4{(uint32_t)(p0 >> 2), 0u, (uint32_t)slot, ctr3(kTagInit, inst)}, k0, k1);
+    const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int p = p0 + q;
+      const uint8_t v = (p < n && (w[q] >> 31)) ? 0xFFu : 0x01u;
+      s8 |= (uint64_t)v << (8 * (half * 4 + q));
+    }
+  }
+  const size_t off = (size_t)slot * n_pos + (size_t)g * kGroup;
+  *reinterpret_cast<uint64_t*>(spins + off) = s8;
+  *reinterpret_cast<uint64_t*>(best_spins + off) = s8;
+}
+
+// Energy of every slot from its spins, in the engine's fixed point, with an order-independent
+// int64 reduction (the integer path accumulates 2E, halved by the finalize kernel).
+template <bool kInt>
+__global__ void energy_fixed_kernel(PtKernelArgs a) {
+  const int S = blockIdx.x, slot = blockIdx.y;
+  const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;  // 256 threads = one slice
+  const int p = S * kSlicePositions + lane * kGroup + q;
+  const int8_t* sp = a.spins + (size_t)slot * a.n_pos;
+  const int w0 = a.slice_off[S], width = a.slice_off[S + 1] - w0;
+  const long long base = (long long)w0 * kSlicePositions + lane;
+  long long v = 0;
+  if (p < a.n) {
+    const int si = sp[p];
+    if constexpr (kInt) {
+      const int8_t* w = static_cast<const int8_t*>(a.ell_w);
+      int f = 0;
+      for (int d = 0; d < width; ++d) {
+        const long long e = base + (long long)(d * kGroup + q) * 32;
+        f += (int)w[e] * (int)sp[a.ell_nbr[e]];
+      }
+      const int hh = static_cast<const int*>(a.h_pos)[(long long)S * kSlicePositions + q * 32 + lane];
+      v = (long long)si * (long long)(-f - 2 * hh);
+    } else {
+      const float* w = static_cast<const float*>(a.ell_w);
+      float f = 0.0f;
+      for (int d = 0; d < width; ++d) {
+        const long long e = base + (long long)(d * kGroup + q) * 32;
+        f = f_add(f, sp[a.ell_nbr[e]] > 0 ? w[e] : -w[e]);
+      }
+      const float hh = static_cast<const float*>(a.h_pos)[(long long)S * kSlicePositions + q * 32 + lane];
+      float term = f_sub(f_mul(-0.5f, f), hh);
+      if (si < 0) term = -term;
+      v = f_to_ll_rn(f_mul(term, kFloatEnergyQuant));
+    }
+  }
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  __shared__ long long red[8];
+  if (lane == 0) red[q] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long s = 0;
+    for (int i = 0; i < 8; ++i) s += red[i];
+    if (s != 0) atomicAdd(reinterpret_cast<unsigned long long*>(a.energy + slot), (unsigned long long)s);
+  }
+}
+
+__global__ void init_finalize_kernel(int R, int halve, long long* energy, long long* best_energy,
+                                     int* rung_of_slot, int* slot_of_rung, long long* tried,
+                                     long long* accepted) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < R; i += gridDim.x * blockDim.x) {
+    if (halve) energy[i] /= 2;  // exact: 2E is even for integer couplings
+    best_energy[i] = energy[i];
+    rung_of_slot[i] = i;
+    slot_of_rung[i] = i;
+    if (i < R - 1) {
+      tried[i] = 0;
+      accepted[i] = 0;
+    }
+  }
+}
+
+// FP64 recompute: E = sum_p s_p (-1/2 sum_j J s_j - h_p), weights and field widened to double.
+template <bool kInt>
+__global__ void energy_fp64_kernel(PtKernelArgs a, const int8_t* spins, double* out) {
+  const int S = blockIdx.x, slot = blockIdx.y;
+  const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
+  const int p = S * kSlicePositions + lane * kGroup + q;
+  const int8_t* sp = spins + (size_t)slot * a.n_pos;
+  const int w0 = a.slice_off[S], width = a.slice_off[S + 1] - w0;
+  const long long base = (long long)w0 * kSlicePositions + lane;
+  double v = 0.0;
+  if (p < a.n) {
+    double f = 0.0, hh;
+    for (int d = 0; d < width; ++d) {
+      const long long e = base + (long long)(d * kGroup + q) * 32;
+      const double wt = kInt ? (double)static_cast<const int8_t*>(a.ell_w)[e] : (double)static_cast<const float*>(a.ell_w)[e];
+      f += wt * (double)sp[a.ell_nbr[e]];
+    }
+    const long long hi = (long long)S * kSlicePositions + q * 32 + lane;
+    hh = kInt ? (double)static_cast<const int*>(a.h_pos)[hi] : (double)static_cast<const float*>(a.h_pos)[hi];
+    v = (double)sp[p] * (-0.5 * f - hh);
+  }
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  __shared__ double red[8];
+  if (lane == 0) red[q] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int i = 0; i < 8; ++i) s += red[i];
+    atomicAdd(out + slot, s);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Launch helpers (called from the C ABI in dpt_capi.cu)
+// ---------------------------------------------------------------------------------------------
+cudaError_t launch_init(const PtKernelArgs& a, int integer_path, cudaStream_t st) {
+  dim3 grid((a.n_pos / kGroup + 127) / 128, a.R);
+  init_spins_kernel<<<grid, 128, 0, st>>>(a.n, a.n_pos, a.R, a.inst, a.k0, a.k1, a.spins, a.best_spins);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(a.energy, 0, sizeof(long long) * a.R, st);
+  if (e != cudaSuccess) return e;
+  dim3 g2(a.n_slices, a.R);
+  if (integer_path) energy_fixed_kernel<true><<<g2, 256, 0, st>>>(a);
+  else energy_fixed_kernel<false><<<g2, 256, 0, st>>>(a);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  init_finalize_kernel<<<(a.R + 255) / 256, 256, 0, st>>>(a.R, integer_path, a.energy, a.best_energy, a.rung_of_slot,
+                                                         a.slot_of_rung, a.tried, a.accepted);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_energy_fp64(const PtKernelArgs& a, int integer_path, const int8_t* spins, int R, double* out,
+                               cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double) * R, st);
+  if (e != cudaSuccess) return e;
+  dim3 g2(a.n_slices, R);
+  if (integer_path) energy_fp64_kernel<true><<<g2, 256, 0, st>>>(a, spins, out);
+  else energy_fp64_kernel<false><<<g2, 256, 0, st>>>(a, spins, out);
+  return cudaGetLastError();
+}
+
+const void* run_kernel_ptr(int integer_path, int in_smem) {
+  if (integer_path) return in_smem ? (const void*)pt_run_kernel<true, true> : (const void*)pt_run_kernel<true, false>;
+  return in_smem ? (const void*)pt_run_kernel<false, true> : (const void*)pt_run_kernel<false, false>;
+}
+
+}  // namespace dpt

@@ -1,0 +1,83 @@
+// dpt_kernels.cuh - kernel argument block and shared-memory plan of the PT kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace dpt {
+
+struct PtKernelArgs {
+  // problem, position space
+  int n, n_pos, n_slices, n_colors, F;
+  long long n_ell;
+  const int* color_ptr;
+  const int* slice_off;
+  const int* ell_nbr;
+  const void* ell_w;
+  const void* h_pos;
+  // ladder and run
+  int R, rpc, spr, n_rounds;
+  long long round0;
+  uint32_t k0, k1, inst;
+  const double* betas;
+  const uint32_t* thr;
+  // state
+  int8_t* spins;
+  long long* energy;
+  long long* best_energy;
+  int8_t* best_spins;
+  int* rung_of_slot;
+  int* slot_of_rung;
+  long long* tried;
+  long long* accepted;
+  double* best_hist;
+  // workspace
+  unsigned long long* bar;
+  int* err;
+  long long* pub;
+  long long timeout_ns;
+};
+
+struct SmemLayout {
+  size_t spins, eacc, ecur, ebest, imp, eall, rung, slot, beta, nb, thr, stats, cptr, ctl;
+  size_t soff, nbr, w, h, total;
+};
+
+__host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+// Byte offsets of every shared-memory array; the host sizes the launch with the same function.
+__host__ __device__ inline SmemLayout smem_layout(int n_pos, int rpc, int R, int F, int n_colors, int n_slices,
+                                                  long long n_ell, bool integer_path, bool ell_in_smem) {
+  SmemLayout L;
+  size_t o = 0;
+  L.spins = o; o = align16(o + (size_t)rpc * n_pos);
+  L.eacc = o;  o = align16(o + 8 * (size_t)rpc);
+  L.ecur = o;  o = align16(o + 8 * (size_t)rpc);
+  L.ebest = o; o = align16(o + 8 * (size_t)rpc);
+  L.imp = o;   o = align16(o + 4 * (size_t)rpc);
+  L.eall = o;  o = align16(o + 8 * (size_t)R);
+  L.rung = o;  o = align16(o + 4 * (size_t)R);
+  L.slot = o;  o = align16(o + 4 * (size_t)R);
+  L.beta = o;  o = align16(o + 8 * (size_t)R);
+  L.nb = o;    o = align16(o + 4 * (size_t)rpc);
+  L.thr = o;   o = align16(o + (integer_path ? 4 * (size_t)R * F : 0));
+  L.stats = o; o = align16(o + 8 * (size_t)(R > 1 ? R - 1 : 0));
+  L.cptr = o;  o = align16(o + 4 * (size_t)(n_colors + 1));
+  L.ctl = o;   o = align16(o + 16);
+  L.soff = L.nbr = L.w = L.h = o;
+  if (ell_in_smem) {
+    L.soff = o; o = align16(o + 4 * (size_t)(n_slices + 1));
+    L.nbr = o;  o = align16(o + 4 * (size_t)n_ell);
+    L.w = o;    o = align16(o + (integer_path ? 1 : 4) * (size_t)n_ell);
+    L.h = o;    o = align16(o + 4 * (size_t)n_pos);
+  }
+  L.total = o;
+  return L;
+}
+
+cudaError_t launch_init(const PtKernelArgs& a, int integer_path, cudaStream_t st);
+cudaError_t launch_energy_fp64(const PtKernelArgs& a, int integer_path, const int8_t* spins, int R, double* out,
+                               cudaStream_t st);
+const void* run_kernel_ptr(int integer_path, int in_smem);
+
+}  // namespace dpt

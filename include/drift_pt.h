@@ -1,0 +1,224 @@
+/* drift_pt.h - C ABI of the B200 parallel-tempering (replica-exchange Metropolis) engine.
+ *
+ * This library replaces the process boundary of DRiFT's GPU path: drift/gpu.py:83-103 writes a
+ * problem.bin, runs the cuda/ising_pt executable as a subprocess and parses result.bin and its
+ * stderr. Here the same inputs (CSR couplings, field, greedy colouring, ladder, rounds, sweeps,
+ * seed) cross a plain C ABI instead: no file, no process, no torch types. Every function returns
+ * an int status (DRIFT_PT_OK = 0) instead of exiting (cuda/ising_pt.cu:30-38); the message of the
+ * last failure on the calling thread is available from drift_pt_last_error().
+ *
+ * Two layers:
+ *   - host helpers (colouring, layout, thresholds) and drift_pt_solve(): host buffers in and out,
+ *     the whole problem.bin -> result.bin contract in one call (it allocates device memory);
+ *   - the device layer (drift_pt_init / drift_pt_run / drift_pt_energy_fp64): every pointer is
+ *     device memory owned by the caller, the call is asynchronous on the given CUDA stream and
+ *     allocates nothing. Scratch space is a caller-provided workspace of
+ *     drift_pt_workspace_bytes() bytes.
+ *
+ * Streams are passed as void* (a cudaStream_t; NULL = legacy default stream).
+ */
+#ifndef DRIFT_PT_H
+#define DRIFT_PT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define DRIFT_PT_API __attribute__((visibility("default")))
+#else
+#define DRIFT_PT_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DRIFT_PT_OK 0
+#define DRIFT_PT_EINVAL 1       /* invalid argument (sizes, pointers, colouring, ladder)        */
+#define DRIFT_PT_ECUDA 2        /* a CUDA runtime call failed                                   */
+#define DRIFT_PT_ETIMEOUT 3     /* a bounded wait inside a kernel gave up (error flag was set)  */
+#define DRIFT_PT_ENOMEM 4       /* device allocation failed (drift_pt_solve only)               */
+#define DRIFT_PT_EUNSUPPORTED 5 /* problem does not fit the engine's limits                     */
+
+/* Version string of the library, e.g. "drift-b200-pt 0.1.0 sm_100a". */
+DRIFT_PT_API const char* drift_pt_version(void);
+
+/* Message of the last failed call on this thread ("" if none). */
+DRIFT_PT_API const char* drift_pt_last_error(void);
+
+/* ---------------------------------------------------------------------------------------------
+ * Problem description in the reference's own terms (drift/gpu.py:66-81): CSR of the symmetric,
+ * zero-diagonal coupling matrix J (rows grouped, columns ascending within a row as np.nonzero
+ * yields them), fp32 weights and field, and a colouring given as color_ptr[k+1] / color_spins[n]
+ * (spin ids grouped by colour, ascending within a colour: the stable argsort of gpu.py:142-144).
+ * ------------------------------------------------------------------------------------------- */
+typedef struct DriftPtCsr {
+  int32_t n;                  /* number of spins                                            */
+  int64_t nnz;                /* directed CSR entries (2 x edges)                           */
+  const int32_t* row_ptr;     /* [n+1]                                                      */
+  const int32_t* col_idx;     /* [nnz]                                                      */
+  const float* weight;        /* [nnz] J_ij                                                 */
+  const float* h;             /* [n]   h_i                                                  */
+  int32_t n_colors;           /* k                                                          */
+  const int32_t* color_ptr;   /* [k+1]                                                      */
+  const int32_t* color_spins; /* [n]                                                        */
+} DriftPtCsr;
+
+/* Greedy colouring in index order, smallest colour unused by an already-coloured neighbour.
+ * Replaces drift/gpu.py:122-141 (_greedy_coloring). color[n] receives each spin's colour. */
+DRIFT_PT_API int drift_pt_greedy_coloring(int32_t n, const int32_t* row_ptr, const int32_t* col_idx,
+                             int32_t* color, int32_t* n_colors);
+
+/* color_ptr[k+1] and color_spins[n] from color[n]: the stable argsort of drift/gpu.py:142-144. */
+DRIFT_PT_API int drift_pt_color_order(int32_t n, const int32_t* color, int32_t n_colors, int32_t* color_ptr,
+                         int32_t* color_spins);
+
+/* ---------------------------------------------------------------------------------------------
+ * Device layout. Spins are renumbered into "positions": colour classes are contiguous position
+ * ranges in color_spins order. Couplings are stored as a sliced ELL: a slice is 256 positions
+ * (32 groups of 8 consecutive positions); its entries are laid out [d][q][lane] where
+ * position = 256*slice + 8*lane + q and d < width(slice) = max degree in the slice. Padded
+ * entries have weight 0. Neighbours keep the CSR (ascending original column) order. Field h is
+ * stored in the same [q][lane] order per slice (width 1).
+ * No counterpart in the reference (its kernel walks the CSR directly, cuda/ising_pt.cu:111-115).
+ * ------------------------------------------------------------------------------------------- */
+typedef struct DriftPtLayoutInfo {
+  int32_t n;                 /* spins                                                       */
+  int32_t n_pos;             /* positions, n rounded up to a multiple of 256                */
+  int32_t n_slices;          /* n_pos / 256                                                 */
+  int32_t n_colors;          /* k                                                           */
+  int64_t n_ell;             /* ELL entries = 256 * sum of slice widths                     */
+  int32_t max_degree;        /* largest row length                                          */
+  int32_t integer_couplings; /* 1 if every J_ij is an integer in [-127,127] and every h_i an
+                                integer in [-2^20, 2^20]                                    */
+  int32_t max_field;         /* F = max_i (sum_j |J_ij| + |h_i|) on the integer path        */
+} DriftPtLayoutInfo;
+
+DRIFT_PT_API int drift_pt_layout_query(const DriftPtCsr* csr, DriftPtLayoutInfo* info);
+
+typedef struct DriftPtLayout { /* caller-allocated arrays, sized from DriftPtLayoutInfo */
+  int32_t* color_ptr;        /* [k+1] position offsets of the colour classes                */
+  int32_t* slice_off;        /* [n_slices+1] offsets in units of 256 entries                */
+  int32_t* ell_nbr;          /* [n_ell] neighbour positions                                 */
+  void* ell_w;               /* [n_ell] int8 (integer path) or float                        */
+  void* h_pos;               /* [n_pos] int32 (integer path) or float, [q][lane] per slice  */
+  int32_t* site_of_pos;      /* [n_pos] original spin id, -1 for padding                    */
+  int32_t* pos_of_site;      /* [n]                                                         */
+} DriftPtLayout;
+
+DRIFT_PT_API int drift_pt_layout_fill(const DriftPtCsr* csr, int32_t integer_path, DriftPtLayout* out);
+
+/* Metropolis thresholds of the integer path, thr[r*F + x-1] = floor(exp(-2 x beta_r) 2^32)
+ * (saturated at 2^32-1) for x = 1..F. Host function. Replaces the per-attempt expf of
+ * cuda/ising_pt.cu:118. */
+DRIFT_PT_API int drift_pt_thresholds(int32_t n_rungs, const double* betas, int32_t max_field, uint32_t* thr);
+
+/* ---------------------------------------------------------------------------------------------
+ * Device layer. All pointers below are device memory.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct DriftPtDeviceProblem {
+  int32_t n, n_pos, n_slices, n_colors;
+  int32_t integer_path;      /* 1: int8 weights, int32 field, threshold table; 0: fp32      */
+  int32_t max_field;         /* F (integer path)                                            */
+  int32_t max_width;         /* largest slice width                                         */
+  int32_t max_class;         /* size of the largest colour class                            */
+  int32_t reserved0;
+  int64_t n_ell;
+  const int32_t* color_ptr;
+  const int32_t* slice_off;
+  const int32_t* ell_nbr;
+  const void* ell_w;
+  const void* h_pos;
+} DriftPtDeviceProblem;
+
+/* Replica state, indexed by replica *slot*. Slots keep their configuration; replica exchange
+ * permutes which rung (beta) each slot holds (rung_of_slot / slot_of_rung). This is the same
+ * Markov chain as swapping configurations between fixed rungs
+ * (drift/solvers/parallel_tempering.py:104-113). */
+typedef struct DriftPtDeviceState {
+  int8_t* spins;             /* [R][n_pos] +-1, position order                              */
+  int64_t* energy;           /* [R] fixed point (scale 1 integer path, 2^-32 float path)    */
+  int64_t* best_energy;      /* [R] lowest energy each slot has held at a round end         */
+  int8_t* best_spins;        /* [R][n_pos]                                                  */
+  int32_t* rung_of_slot;     /* [R]                                                         */
+  int32_t* slot_of_rung;     /* [R]                                                         */
+  int64_t* swap_tried;       /* [R-1] per rung pair (r, r+1), cumulative                    */
+  int64_t* swap_accepted;    /* [R-1]                                                       */
+  double* best_history;      /* [n_rounds of a run] best energy so far after each round, or NULL */
+} DriftPtDeviceState;
+
+typedef struct DriftPtRunArgs {
+  int32_t n_replicas;        /* R (rungs = slots)                                           */
+  int32_t n_rounds;          /* rounds in this call                                         */
+  int32_t sweeps_per_round;  /* Metropolis sweeps between exchange steps                    */
+  int32_t reserved0;
+  int64_t round_offset;      /* index of the first round (resume); sweeps are numbered
+                                round * sweeps_per_round + j                                */
+  uint64_t seed;
+  uint32_t instance;         /* stream id (< 2^24), distinct per independent chain set      */
+  int32_t replicas_per_cta;  /* 0 = auto (autotuner)                                        */
+  int32_t threads_per_cta;   /* 0 = auto                                                    */
+  int32_t reserved1;
+  const double* betas;       /* [R] inverse temperature of each rung                        */
+  const uint32_t* thresholds;/* [R][F] integer path (from drift_pt_thresholds), else NULL   */
+  double timeout_s;          /* bound on any in-kernel wait (0 = 10 s)                      */
+} DriftPtRunArgs;
+
+/* Bytes of device workspace drift_pt_run needs for R replicas. */
+DRIFT_PT_API int drift_pt_workspace_bytes(int32_t n_replicas, size_t* bytes);
+
+/* Random initial spins (Philox, seed/instance of args), their energies, best = initial,
+ * identity rung assignment, zeroed swap counters. Asynchronous. */
+DRIFT_PT_API int drift_pt_init(const DriftPtDeviceProblem* prob, const DriftPtRunArgs* args,
+                  DriftPtDeviceState* state, void* stream);
+
+/* Runs args->n_rounds rounds of (sweeps_per_round colour-ordered Metropolis sweeps on every
+ * replica, then one exchange step over adjacent rungs with parity = round & 1). Replaces the
+ * host loop of cuda/ising_pt.cu:214-218 with one persistent launch. Asynchronous; the
+ * workspace must not be shared with a concurrent call. Call drift_pt_check() to learn whether
+ * a bounded wait timed out. */
+DRIFT_PT_API int drift_pt_run(const DriftPtDeviceProblem* prob, const DriftPtRunArgs* args,
+                 DriftPtDeviceState* state, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Synchronises the stream and returns DRIFT_PT_ETIMEOUT if the workspace's error flag is set. */
+DRIFT_PT_API int drift_pt_check(void* workspace, void* stream);
+
+/* Full recompute of every slot's energy in FP64 from its spins (the check on the incremental
+ * bookkeeping; cuda/ising_pt.cu:59-68 computes it at init only). out[R] in the model's units. */
+DRIFT_PT_API int drift_pt_energy_fp64(const DriftPtDeviceProblem* prob, const int8_t* spins, int32_t n_replicas,
+                         double* out, void* stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Host convenience: one call from host buffers to host results (the problem.bin -> result.bin
+ * contract of cuda/ising_pt.cu:159-243 and drift/gpu.py:83-114). Allocates and frees device
+ * memory internally; synchronous.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct DriftPtSolveArgs {
+  int32_t n_replicas;
+  int32_t n_rounds;
+  int32_t sweeps_per_round;
+  int32_t reserved0;
+  uint64_t seed;
+  double T_min, T_max;       /* geometric ladder (drift/solvers/parallel_tempering.py:29-36) */
+  const double* betas;       /* optional explicit ladder [R] (host), overrides T_min/T_max  */
+} DriftPtSolveArgs;
+
+typedef struct DriftPtSolveResult { /* caller-allocated host buffers; optional ones may be NULL */
+  double best_E;
+  double seconds;            /* device time of the round loop                               */
+  double throughput;         /* attempts per second = R * n_rounds * sweeps * n / seconds   */
+  double swap_rate;          /* accepted / tried over all exchange attempts                 */
+  float* best_s;             /* [n] +-1 of the lowest-energy configuration seen             */
+  int8_t* rung_spins;        /* [R][n] optional: final configuration at each rung           */
+  double* rung_energy;       /* [R] optional: final energy at each rung                     */
+  int64_t* swap_tried;       /* [R-1] optional                                              */
+  int64_t* swap_accepted;    /* [R-1] optional                                              */
+  double* best_history;      /* [n_rounds] optional                                         */
+} DriftPtSolveResult;
+
+DRIFT_PT_API int drift_pt_solve(const DriftPtCsr* csr, const DriftPtSolveArgs* args, DriftPtSolveResult* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DRIFT_PT_H */

@@ -1,0 +1,207 @@
+"""Parity of the sm_100a engine with the oracle, through the C ABI (GPU required).
+
+Bit-exact: final spins of every replica slot, fixed-point energies, per-slot best energies and
+configurations, the rung permutation, per-pair exchange counts and the best-energy history, on
+integer (+-J, MaxCut) and fp32 (Gaussian field / couplings) problems, for every launch shape,
+and across resumed runs. Also: the reference's own GPU acceptance checks (tests/test_gpu.py,
+tests/test_parallel_tempering.py of the reference) through the drop-in parallel_tempering_gpu.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import cuda_ready, dense_from_edges
+
+from drift_b200 import _lib
+from drift_b200.engine import DeviceProblem, HostProblem, PtEngine, geometric_betas
+from drift_b200.gpu import parallel_tempering_gpu
+from drift_b200.instances import ea_2d, er_gaussian, maxcut_3regular, pm_spin_glass, random_graph, maxcut_ising, sk_model
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not cuda_ready(), reason="needs CUDA and libdrift_pt.so")]
+
+
+def oracle_problem(hp: HostProblem, integer_path: bool):
+    return oracle.OracleProblem(hp.n, hp.row_ptr, hp.col_idx, hp.weight, hp.h, hp.color_ptr, hp.color_spins,
+                                integer_path=integer_path)
+
+
+def run_engine(model, betas, rounds, spr, seed, *, rpc=0, threads=0, instance=0, chunks=None, integer_path=None):
+    import torch
+
+    hp = HostProblem.from_model(model)
+    prob = DeviceProblem(hp, integer_path=integer_path)
+    eng = PtEngine(prob, betas, seed=seed, sweeps_per_round=spr, instance=instance, replicas_per_cta=rpc,
+                   threads_per_cta=threads)
+    eng.init()
+    hist = torch.zeros(max(rounds, 1), dtype=torch.float64, device="cuda")
+    done = 0
+    for c in (chunks or [rounds]):
+        eng.run(c, history=hist[done:])
+        done += c
+    eng.check()
+    return hp, prob, eng, eng.fetch(), hist.cpu().numpy()[:rounds]
+
+
+def assert_bit_exact(st, ost, hist, rounds):
+    assert np.array_equal(st["spins"], ost.spins)
+    assert np.array_equal(st["energy_fixed"], ost.energy)
+    assert np.array_equal(st["best_energy_fixed"], ost.best_energy)
+    assert np.array_equal(st["best_spins"], ost.best_spins)
+    assert np.array_equal(st["rung_of_slot"], ost.rung_of_slot)
+    assert np.array_equal(st["slot_of_rung"], ost.slot_of_rung)
+    R = len(ost.energy)
+    assert np.array_equal(st["tried"], ost.tried[: R - 1])
+    assert np.array_equal(st["accepted"], ost.accepted[: R - 1])
+    assert np.array_equal(hist, ost.best_history[:rounds])
+
+
+CASES = {
+    # name: (model factory, R, (beta_hot, beta_cold) or T range, rounds, sweeps_per_round, seed)
+    "ferro_chain_18": (lambda: dense_from_edges(18, {"i": list(range(17)), "j": list(range(1, 18)), "w": [1.0] * 17},
+                                                [0.0] * 18), 12, (0.05, 3.0), 150, 4, 0),
+    "maxcut_g16_s3": (lambda: maxcut_ising(random_graph(16, 0.5, 3)), 16, (0.05, 4.0), 200, 4, 1),
+    "glass_n14_field_fp32": (lambda: pm_spin_glass(14, 7, field=0.3), 20, (0.05, 5.0), 300, 5, 2),
+    "ea2d_L16_C1": (lambda: ea_2d(16, 1), 24, (1 / 3.0, 10.0), 2000, 1, 1),
+    "maxcut_3reg_4096_C2": (lambda: maxcut_3regular(4096, 2), 64, (0.25, 5.0), 25, 4, 7),
+    "er_gaussian_2000_fp32": (lambda: er_gaussian(2000, 6, 3), 8, (1 / 3.0, 10.0), 12, 2, 3),
+    "sk_64_dense_fp32": (lambda: sk_model(64, 4), 8, (1 / 3.0, 1 / 0.3), 40, 2, 4),
+}
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_engine_matches_oracle_bit_exact(name):
+    make, R, (tmin, tmax), rounds, spr, seed = CASES[name]
+    model = make()
+    betas = geometric_betas(R, tmin, tmax)
+    hp, prob, eng, st, hist = run_engine(model, betas, rounds, spr, seed)
+    ost = oracle.pt_run(oracle_problem(hp, prob.integer_path), betas, n_rounds=rounds, sweeps_per_round=spr,
+                        seed=seed, thr=eng.thr)
+    assert_bit_exact(st, ost, hist, rounds)
+
+
+@pytest.mark.parametrize("rpc,threads", [(1, 64), (1, 1024), (2, 256), (8, 512), (64, 1024)])
+def test_results_do_not_depend_on_launch_shape(rpc, threads):
+    model = maxcut_3regular(2048, 5)
+    R, rounds, spr, seed = 64, 10, 2, 11
+    betas = geometric_betas(R, 0.25, 5.0)
+    hp, prob, eng, st, hist = run_engine(model, betas, rounds, spr, seed, rpc=rpc, threads=threads)
+    ost = oracle.pt_run(oracle_problem(hp, True), betas, n_rounds=rounds, sweeps_per_round=spr, seed=seed, thr=eng.thr)
+    assert_bit_exact(st, ost, hist, rounds)
+
+
+def test_fp32_path_launch_shapes_and_resume():
+    model = er_gaussian(1500, 6, 9)
+    R, spr, seed = 16, 3, 5
+    betas = geometric_betas(R, 1 / 3.0, 10.0)
+    chunks = [3, 1, 6]
+    hp, prob, eng, st, hist = run_engine(model, betas, sum(chunks), spr, seed, rpc=4, threads=128, chunks=chunks)
+    ost = oracle.pt_run(oracle_problem(hp, False), betas, n_rounds=sum(chunks), sweeps_per_round=spr, seed=seed)
+    assert_bit_exact(st, ost, hist, sum(chunks))
+
+
+def test_resume_equals_single_run_integer():
+    model = ea_2d(24, 3)
+    R, spr, seed = 10, 2, 4
+    betas = geometric_betas(R, 0.4, 3.0)
+    chunks = [7, 13, 1, 9]
+    hp, prob, eng, st, hist = run_engine(model, betas, sum(chunks), spr, seed, chunks=chunks)
+    ost = oracle.pt_run(oracle_problem(hp, True), betas, n_rounds=sum(chunks), sweeps_per_round=spr, seed=seed,
+                        thr=eng.thr)
+    assert_bit_exact(st, ost, hist, sum(chunks))
+
+
+def test_integer_couplings_forced_onto_fp32_path_match_oracle():
+    model = ea_2d(16, 2)
+    betas = geometric_betas(8, 0.3, 3.0)
+    hp, prob, eng, st, hist = run_engine(model, betas, 30, 2, 3, integer_path=False)
+    ost = oracle.pt_run(oracle_problem(hp, False), betas, n_rounds=30, sweeps_per_round=2, seed=3)
+    assert_bit_exact(st, ost, hist, 30)
+
+
+def test_instance_id_selects_an_independent_stream():
+    model = maxcut_3regular(512, 1)
+    betas = geometric_betas(8, 0.25, 5.0)
+    _, _, eng0, st0, _ = run_engine(model, betas, 5, 2, 3, instance=0)
+    hp, _, eng5, st5, hist = run_engine(model, betas, 5, 2, 3, instance=5)
+    assert not np.array_equal(st0["spins"], st5["spins"])
+    ost = oracle.pt_run(oracle_problem(hp, True), betas, n_rounds=5, sweeps_per_round=2, seed=3, instance=5, thr=eng5.thr)
+    assert_bit_exact(st5, ost, hist, 5)
+
+
+def test_energy_bookkeeping_against_fp64_recompute():
+    # integer path: the incremental int64 energy equals the FP64 recompute exactly
+    _, _, eng, st, _ = run_engine(maxcut_3regular(4096, 2), geometric_betas(16, 0.25, 5.0), 50, 4, 1)
+    assert np.array_equal(eng.energy_fp64(), st["energy_fixed"].astype(np.float64))
+    # fp32 path: fixed-point bookkeeping stays within 1e-5 relative of FP64 after 20k flips/spin
+    model = er_gaussian(3000, 6, 4)
+    _, _, eng, st, _ = run_engine(model, geometric_betas(8, 1 / 3.0, 10.0), 200, 100, 2)
+    e64 = eng.energy_fp64()
+    assert np.all(np.abs(st["energy"] - e64) <= 1e-5 * (1.0 + np.abs(e64)))
+    for r in range(8):
+        assert model.energy(st["spins"][r]) == pytest.approx(e64[r], rel=1e-9, abs=1e-9)
+
+
+# ---- the reference's acceptance checks through the drop-in ----------------------------------
+
+def test_gpu_reproduces_exact_on_small_maxcut(reference_instances):
+    """tests/test_gpu.py:45-54 of the reference."""
+    d = reference_instances["maxcut_g12_p05_s3"]
+    model = dense_from_edges(d["n"], d["edges"], d["h"])
+    res = parallel_tempering_gpu(model, n_replicas=16, T_min=0.05, T_max=4.0, n_rounds=200, sweeps_per_round=4,
+                                 seed=1)
+    assert res.best_E == pytest.approx(d["e_exact"])
+    assert model.energy(res.best_s) == pytest.approx(res.best_E)
+    assert 0.0 < res.swap_rate < 1.0 and res.throughput > 0 and res.seconds > 0
+    assert len(res.best_history) == 200 and res.best_history[-1] == pytest.approx(res.best_E)
+
+
+@pytest.mark.parametrize("name,kw", [
+    ("maxcut_g16_p05_s3", dict(n_replicas=16, T_min=0.05, T_max=4.0, n_rounds=200, sweeps_per_round=4, seed=1)),
+    ("maxcut_g18_p04_s8", dict(n_replicas=16, T_min=0.05, T_max=4.0, n_rounds=200, sweeps_per_round=4, seed=1)),
+    ("glass_n14_s7_field", dict(n_replicas=20, T_min=0.05, T_max=5.0, n_rounds=300, sweeps_per_round=5, seed=2)),
+    ("ferro_n18", dict(n_replicas=12, T_min=0.05, T_max=3.0, n_rounds=150, sweeps_per_round=4, seed=0)),
+    ("maxcut_g20_p05_s2", dict(n_replicas=16, n_rounds=80, sweeps_per_round=4, seed=1)),
+])
+def test_drop_in_finds_exact_ground_states(reference_instances, name, kw):
+    """tests/test_parallel_tempering.py:37-68 and experiments/phase14_gpu.py:38-65 of the reference."""
+    d = reference_instances[name]
+    model = dense_from_edges(d["n"], d["edges"], d["h"])
+    res = parallel_tempering_gpu(model, **kw)
+    assert np.isclose(res.best_E, d["e_exact"]), f"GPU PT {res.best_E} != exact {d['e_exact']}"
+    assert res.rung_spins.shape == (kw["n_replicas"], d["n"])
+    for r in range(kw["n_replicas"]):
+        assert model.energy(res.rung_spins[r]) == pytest.approx(res.rung_energies[r], abs=1e-4)
+
+
+def test_solve_abi_matches_device_layer():
+    """drift_pt_solve (host buffers in and out) runs the same chain as the device layer."""
+    model = maxcut_3regular(1024, 4)
+    R, rounds, spr, seed = 32, 20, 3, 8
+    hp = HostProblem.from_model(model)
+    betas = geometric_betas(R, 0.25, 5.0)
+    _, _, eng, st, hist = run_engine(model, betas, rounds, spr, seed)
+    L = _lib.load()
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    best_s = np.zeros(hp.n, np.float32)
+    rung_spins = np.zeros((R, hp.n), np.int8)
+    rung_e = np.zeros(R)
+    tried = np.zeros(R - 1, np.int64)
+    acc = np.zeros(R - 1, np.int64)
+    bh = np.zeros(rounds)
+    args = _lib.SolveArgs(R, rounds, spr, 0, seed, 0.0, 0.0, p(betas))
+    res = _lib.SolveResult(0, 0, 0, 0, p(best_s), p(rung_spins), p(rung_e), p(tried), p(acc), p(bh))
+    _lib.check(L.drift_pt_solve(C.byref(hp.c_csr()), C.byref(args), C.byref(res)), "drift_pt_solve")
+    assert np.array_equal(tried, st["tried"]) and np.array_equal(acc, st["accepted"])
+    assert np.array_equal(bh, hist)
+    slot = st["slot_of_rung"]
+    assert np.array_equal(rung_spins, st["spins"][slot])
+    assert np.array_equal(rung_e, st["energy"][slot])
+    b = int(np.argmin(st["best_energy_fixed"]))
+    assert np.array_equal(best_s, st["best_spins"][b].astype(np.float32))
+    assert res.best_E == pytest.approx(model.energy(best_s.astype(np.float64)))
+    assert res.throughput > 0 and 0.0 < res.swap_rate < 1.0
