@@ -32,7 +32,7 @@ class Csr(C.Structure):
 class LayoutInfo(C.Structure):
     _fields_ = [("n", C.c_int32), ("n_pos", C.c_int32), ("n_slices", C.c_int32), ("n_colors", C.c_int32),
                 ("n_ell", C.c_int64), ("max_degree", C.c_int32), ("integer_couplings", C.c_int32),
-                ("max_field", C.c_int32)]
+                ("max_field", C.c_int32), ("has_field", C.c_int32)]
 
 
 class Layout(C.Structure):
@@ -43,7 +43,7 @@ class Layout(C.Structure):
 class DeviceProblem(C.Structure):
     _fields_ = [("n", C.c_int32), ("n_pos", C.c_int32), ("n_slices", C.c_int32), ("n_colors", C.c_int32),
                 ("integer_path", C.c_int32), ("max_field", C.c_int32), ("max_width", C.c_int32),
-                ("max_class", C.c_int32), ("reserved0", C.c_int32), ("n_ell", C.c_int64),
+                ("max_class", C.c_int32), ("has_field", C.c_int32), ("n_ell", C.c_int64),
                 ("color_ptr", vp), ("slice_off", vp), ("ell_nbr", vp), ("ell_w", vp), ("h_pos", vp)]
 
 

@@ -126,36 +126,63 @@ int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPl
   if (rc) return rc;
   const int R = r->n_replicas;
   const int ip = p->integer_path;
-  auto total = [&](int rpc, bool ell) {
-    return smem_layout(p->n_pos, rpc, R, p->max_field, p->n_colors, p->n_slices, p->n_ell, ip != 0, ell).total;
+  auto total = [&](int rpc, bool ell, int threads) {
+    return smem_layout(p->n_pos, rpc, R, p->max_field, p->n_colors, p->n_slices, p->n_ell, ip != 0, ell, threads)
+        .total;
+  };
+  // threads per slot: one per group of 8 positions of the largest colour class, as a power of
+  // two below 32 or a multiple of 32, with rpc * tps a multiple of 32 and at most 1024 (0 = none)
+  const int want = p->max_class / kGroup + 2;
+  auto pick_tps = [&](int rpc) -> int {
+    int tps = 1;
+    while (tps < 32 && tps < want) tps *= 2;
+    if (tps >= 32) tps = ((want + 31) / 32) * 32;
+    while (rpc * tps > 1024 && tps > 1) tps = tps > 32 ? tps - 32 : tps / 2;
+    while ((rpc * tps) % 32 != 0) {
+      tps = tps < 32 ? tps * 2 : tps + 32;
+      if (rpc * tps > 1024) return 0;
+    }
+    return rpc * tps <= 1024 ? tps : 0;
   };
   int rpc = r->replicas_per_cta;
   if (rpc <= 0) {
-    // Work of one round on one replica vs the cost of a grid-wide barrier (~1-2 us): small
+    // Work of one round on one replica vs the cost of a grid-wide barrier (~5 us): small
     // problems keep every replica in one CTA and need no barrier at all.
     const double work = (double)R * p->n * std::max(1, r->sweeps_per_round);
-    if (work <= 65536.0 && total(R, false) <= (size_t)di.max_smem_optin) rpc = R;
-    else rpc = 1;
+    if (work <= 65536.0 && R <= 1024 && pick_tps(R) > 0 && total(R, false, R * pick_tps(R)) <= (size_t)di.max_smem_optin)
+      rpc = R;
+    else
+      rpc = 1;
+    while (rpc < R && (R + rpc - 1) / rpc > di.sm_count) rpc *= 2;
+    rpc = std::min(rpc, R);
+    while (rpc > 1 && pick_tps(rpc) == 0) rpc /= 2;
   }
   rpc = std::min(rpc, R);
-  while (rpc < R && (R + rpc - 1) / rpc > di.sm_count) rpc *= 2;
-  rpc = std::min(rpc, R);
-  if (total(rpc, false) > (size_t)di.max_smem_optin)
-    return set_error(DRIFT_PT_EUNSUPPORTED, "replica state of %d x %d positions exceeds shared memory (%d B)", rpc,
-                     p->n_pos, di.max_smem_optin);
-  const bool in_smem = total(rpc, true) <= (size_t)di.max_smem_optin;
+  if ((R + rpc - 1) / rpc > 65535) return set_error(DRIFT_PT_EUNSUPPORTED, "too many CTAs");
   int threads = r->threads_per_cta;
   if (threads <= 0) {
-    const int groups = p->max_class / kGroup + 2;
-    threads = std::min(1024, std::max(64, ((rpc * groups + 31) / 32) * 32));
+    const int tps = pick_tps(rpc);
+    if (tps == 0) return set_error(DRIFT_PT_EUNSUPPORTED, "no launch shape for %d replicas per CTA", rpc);
+    threads = rpc * tps;
   }
-  if (threads < 32 || threads > 1024 || threads % 32) return set_error(DRIFT_PT_EINVAL, "threads_per_cta must be a multiple of 32 in [32, 1024]");
+  {
+    const int tps = threads / rpc;
+    const bool pow2 = tps > 0 && (tps & (tps - 1)) == 0;
+    if (threads < 32 || threads > 1024 || threads % 32 || threads % rpc || !(tps % 32 == 0 || (tps < 32 && pow2)))
+      return set_error(DRIFT_PT_EINVAL,
+                       "threads_per_cta (%d) must be a multiple of 32 in [32, 1024] and of replicas_per_cta (%d), "
+                       "with threads/replica a power of two below 32 or a multiple of 32", threads, rpc);
+  }
+  if (total(rpc, false, threads) > (size_t)di.max_smem_optin)
+    return set_error(DRIFT_PT_EUNSUPPORTED, "replica state of %d x %d positions exceeds shared memory (%d B)", rpc,
+                     p->n_pos, di.max_smem_optin);
+  const bool in_smem = total(rpc, true, threads) <= (size_t)di.max_smem_optin;
   lp->rpc = rpc;
   lp->threads = threads;
   lp->in_smem = in_smem ? 1 : 0;
   lp->grid = (R + rpc - 1) / rpc;
-  lp->smem = total(rpc, in_smem);
-  const void* fn = run_kernel_ptr(ip, lp->in_smem);
+  lp->smem = total(rpc, in_smem, threads);
+  const void* fn = run_kernel_ptr(ip, lp->in_smem, p->max_width, p->has_field);
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lp->smem);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
   int per_sm = 0;
@@ -212,7 +239,7 @@ extern "C" int drift_pt_run(const DriftPtDeviceProblem* prob, const DriftPtRunAr
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   void* kargs[] = {&a};
-  e = cudaLaunchKernelExC(&cfg, run_kernel_ptr(prob->integer_path, lp.in_smem), kargs);
+  e = cudaLaunchKernelExC(&cfg, run_kernel_ptr(prob->integer_path, lp.in_smem, prob->max_width, prob->has_field), kargs);
   if (e != cudaSuccess) return cuda_fail(e, "pt_run_kernel launch");
   return DRIFT_PT_OK;
 }
@@ -340,6 +367,7 @@ extern "C" int drift_pt_solve(const DriftPtCsr* csr, const DriftPtSolveArgs* arg
   prob.max_field = info.max_field;
   prob.max_width = info.max_degree;
   prob.max_class = max_class;
+  prob.has_field = info.has_field;
   prob.n_ell = info.n_ell;
   prob.color_ptr = reinterpret_cast<const int32_t*>(d + o_cp);
   prob.slice_off = reinterpret_cast<const int32_t*>(d + o_so);

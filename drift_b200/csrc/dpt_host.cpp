@@ -168,6 +168,12 @@ extern "C" int drift_pt_layout_query(const DriftPtCsr* csr, DriftPtLayoutInfo* i
     F = std::max(F, f);
   }
   if (integer && F > (1 << 24)) integer = false;
+  info->has_field = 0;
+  for (int32_t i = 0; i < n; ++i)
+    if (csr->h[i] != 0.0f) {
+      info->has_field = 1;
+      break;
+    }
   info->integer_couplings = integer ? 1 : 0;
   info->max_field = integer ? (int32_t)std::max<int64_t>(F, 1) : 0;
   return DRIFT_PT_OK;

@@ -40,88 +40,155 @@ __device__ __forceinline__ int ld_relaxed_i32(const int* p) {
   return v;
 }
 
-template <bool kInSmem, typename T>
-__device__ __forceinline__ T ld_table(const T* p) {
+// ---------------------------------------------------------------------------------------------
+// One item: positions 8g .. 8g+7 of one replica slot; positions outside the colour range
+// [lo, hi) are computed but never flipped. All gathers of the item are issued before the
+// acceptance tests (W bounds the slice width at compile time; W = 0 walks it at run time).
+// ---------------------------------------------------------------------------------------------
+struct Tables {
+  const int* soff;        // slice offsets
+  const uint32_t* ent;    // shared-memory integer path: neighbour | weight << 24
+  const int* nbr;         // neighbour positions (float path, or global integer path)
+  const int8_t* w8;       // global integer path weights
+  const float* wf;        // float path weights
+  const void* h;          // field, [slice][q][lane]
+};
+
+template <bool kInSmem>
+__device__ __forceinline__ void load_int_entry(const Tables& T, uint32_t e, int& nb, int& w) {
+  if constexpr (kInSmem) {
+    const uint32_t v = T.ent[e];
+    nb = (int)(v & 0xFFFFFFu);
+    w = ((int)v) >> 24;
+  } else {
+    nb = __ldg(T.nbr + e);
+    w = (int)__ldg(T.w8 + e);
+  }
+}
+
+template <bool kInSmem>
+__device__ __forceinline__ int ld_int(const int* p) {
   if constexpr (kInSmem) return *p;
   else return __ldg(p);
 }
 
-// ---------------------------------------------------------------------------------------------
-// One item: positions 8g .. 8g+7 of one replica slot, restricted to colour range [lo, hi).
-// ---------------------------------------------------------------------------------------------
-template <bool kInt, bool kInSmem>
-__device__ __forceinline__ long long sweep_group(int g, int lo, int hi, uint32_t t, int slot,
-                                                 int8_t* __restrict__ sp,
-                                                 const int* __restrict__ soff,
-                                                 const int* __restrict__ nbr,
-                                                 const void* __restrict__ wv,
-                                                 const void* __restrict__ hv,
-                                                 const uint32_t* __restrict__ thr_rung, int F,
-                                                 float neg2beta, uint32_t inst, uint32_t k0,
-                                                 uint32_t k1) {
-  const U4 rnd = philox(U4{(uint32_t)g, t, (uint32_t)slot, ctr3(kTagSweep, inst)}, k0, k1);
+template <int W, bool kInSmem, bool kField>
+__device__ __forceinline__ int group_int(int g, int lo, int hi, uint32_t t, uint32_t slot, int8_t* __restrict__ sp,
+                                         const Tables& T, const uint32_t* __restrict__ thr_rung, int F,
+                                         uint32_t c_sweep, uint32_t c_second, uint32_t k0, uint32_t k1) {
+  const U4 rnd = philox(U4{(uint32_t)g, t, slot, c_sweep}, k0, k1);
   const uint32_t words[4] = {rnd.x, rnd.y, rnd.z, rnd.w};
-  uint64_t s8 = *reinterpret_cast<const uint64_t*>(sp + (size_t)g * kGroup);
+  uint64_t s8 = *reinterpret_cast<const uint64_t*>(sp + g * kGroup);
   const int S = g >> 5, lane = g & 31;
-  const int w0 = ld_table<kInSmem>(soff + S), w1 = ld_table<kInSmem>(soff + S + 1);
-  const int width = w1 - w0;
-  const long long base = (long long)w0 * kSlicePositions + lane;
-  const long long hbase = (long long)S * kSlicePositions + lane;
+  const int w0 = ld_int<kInSmem>(T.soff + S);
+  const int width = ld_int<kInSmem>(T.soff + S + 1) - w0;
+  const uint32_t base = (uint32_t)w0 * kSlicePositions + lane;
+  int field[kGroup];
+#pragma unroll
+  for (int q = 0; q < kGroup; ++q)
+    field[q] = kField ? ld_int<kInSmem>(static_cast<const int*>(T.h) + S * kSlicePositions + q * 32 + lane) : 0;
+  auto step = [&](int d) {
+    int nb[kGroup], wt[kGroup];
+#pragma unroll
+    for (int q = 0; q < kGroup; ++q) load_int_entry<kInSmem>(T, base + (uint32_t)d * kSlicePositions + q * 32, nb[q], wt[q]);
+#pragma unroll
+    for (int q = 0; q < kGroup; ++q) field[q] += wt[q] * (int)sp[nb[q]];
+  };
+  if constexpr (W > 0) {
+#pragma unroll
+    for (int d = 0; d < W; ++d)
+      if (d < width) step(d);
+  } else {
+    for (int d = 0; d < width; ++d) step(d);
+  }
+  int dacc = 0;
+#pragma unroll
+  for (int q = 0; q < kGroup; ++q) {
+    const int p = g * kGroup + q;
+    const int si = (int)(int8_t)(uint8_t)(s8 >> (8 * q));
+    const int x = si * field[q];
+    const bool in = (p >= lo) & (p < hi);
+    const uint32_t thr = thr_rung[min(max(x, 1), F) - 1];
+    const uint32_t prim = (words[q >> 1] >> ((q & 1) * 16)) & 0xFFFFu;
+    const uint32_t th = thr >> 16;
+    bool acc = (x <= 0) | (prim < th);
+    if (in & (x > 0) & (prim == th)) {  // the first 16 bits tie: draw the second half of this uniform
+      const U4 r2 = philox(U4{(uint32_t)p, t, slot, c_second}, k0, k1);
+      acc = (r2.x & 0xFFFFu) < (thr & 0xFFFFu);
+    }
+    acc = acc & in;
+    s8 ^= acc ? ((uint64_t)0xFEu << (8 * q)) : 0ull;  // +1 (0x01) <-> -1 (0xFF)
+    dacc += acc ? 2 * x : 0;
+  }
+  *reinterpret_cast<uint64_t*>(sp + g * kGroup) = s8;
+  return dacc;
+}
+
+template <int W, bool kInSmem, bool kField>
+__device__ __forceinline__ long long group_f32(int g, int lo, int hi, uint32_t t, uint32_t slot,
+                                               int8_t* __restrict__ sp, const Tables& T, float neg2beta,
+                                               uint32_t c_sweep, uint32_t c_second, uint32_t k0, uint32_t k1) {
+  const U4 rnd = philox(U4{(uint32_t)g, t, slot, c_sweep}, k0, k1);
+  const uint32_t words[4] = {rnd.x, rnd.y, rnd.z, rnd.w};
+  uint64_t s8 = *reinterpret_cast<const uint64_t*>(sp + g * kGroup);
+  const int S = g >> 5, lane = g & 31;
+  const int w0 = ld_int<kInSmem>(T.soff + S);
+  const int width = ld_int<kInSmem>(T.soff + S + 1) - w0;
+  const uint32_t base = (uint32_t)w0 * kSlicePositions + lane;
+  float field[kGroup];
+#pragma unroll
+  for (int q = 0; q < kGroup; ++q) {
+    const float* hp = static_cast<const float*>(T.h) + S * kSlicePositions + q * 32 + lane;
+    field[q] = kField ? (kInSmem ? *hp : __ldg(hp)) : 0.0f;
+  }
+  auto step = [&](int d) {
+    int nb[kGroup];
+    float wt[kGroup];
+#pragma unroll
+    for (int q = 0; q < kGroup; ++q) {
+      const uint32_t e = base + (uint32_t)d * kSlicePositions + q * 32;
+      nb[q] = ld_int<kInSmem>(T.nbr + e);
+      wt[q] = kInSmem ? T.wf[e] : __ldg(T.wf + e);
+    }
+#pragma unroll
+    for (int q = 0; q < kGroup; ++q) field[q] = f_add(field[q], sp[nb[q]] > 0 ? wt[q] : -wt[q]);
+  };
+  if constexpr (W > 0) {
+#pragma unroll
+    for (int d = 0; d < W; ++d)
+      if (d < width) step(d);
+  } else {
+    for (int d = 0; d < width; ++d) step(d);
+  }
   long long dacc = 0;
 #pragma unroll
   for (int q = 0; q < kGroup; ++q) {
     const int p = g * kGroup + q;
-    if (p < lo || p >= hi) continue;
     const int si = (int)(int8_t)(uint8_t)(s8 >> (8 * q));
-    bool acc;
-    uint32_t thr = 0;
-    long long dE = 0;
-    if constexpr (kInt) {
-      const int8_t* w = static_cast<const int8_t*>(wv);
-      int field = ld_table<kInSmem>(static_cast<const int*>(hv) + hbase + q * 32);
-      for (int d = 0; d < width; ++d) {
-        const long long e = base + (long long)(d * kGroup + q) * 32;
-        field += (int)ld_table<kInSmem>(w + e) * (int)sp[ld_table<kInSmem>(nbr + e)];
-      }
-      int x = si * field;
-      acc = (x <= 0);
-      if (!acc) thr = thr_rung[min(x, F) - 1];
-      dE = 2LL * x;
-    } else {
-      const float* w = static_cast<const float*>(wv);
-      float field = ld_table<kInSmem>(static_cast<const float*>(hv) + hbase + q * 32);
-      for (int d = 0; d < width; ++d) {
-        const long long e = base + (long long)(d * kGroup + q) * 32;
-        const float wt = ld_table<kInSmem>(w + e);
-        field = f_add(field, sp[ld_table<kInSmem>(nbr + e)] > 0 ? wt : -wt);
-      }
-      const float x = si > 0 ? field : -field;
-      acc = !(x > 0.0f);
-      if (!acc) thr = threshold_f(neg2beta, x);
-      dE = f_to_ll_rn(f_mul(x, 2.0f * kFloatEnergyQuant));
+    const float x = si > 0 ? field[q] : -field[q];
+    const bool in = (p >= lo) & (p < hi);
+    const bool pos = x > 0.0f;
+    const uint32_t thr = threshold_f(neg2beta, pos ? x : 0.0f);
+    const uint32_t prim = (words[q >> 1] >> ((q & 1) * 16)) & 0xFFFFu;
+    const uint32_t th = thr >> 16;
+    bool acc = (!pos) | (prim < th);
+    if (in & pos & (prim == th)) {
+      const U4 r2 = philox(U4{(uint32_t)p, t, slot, c_second}, k0, k1);
+      acc = (r2.x & 0xFFFFu) < (thr & 0xFFFFu);
     }
-    if (!acc) {
-      const uint32_t prim = (words[q >> 1] >> ((q & 1) * 16)) & 0xFFFFu;
-      const uint32_t th = thr >> 16;
-      acc = prim < th;
-      if (prim == th) {  // the first 16 bits tie: draw the second half of this uniform
-        const U4 r2 = philox(U4{(uint32_t)p, t, (uint32_t)slot, ctr3(kTagSecond, inst)}, k0, k1);
-        acc = (r2.x & 0xFFFFu) < (thr & 0xFFFFu);
-      }
-    }
-    if (acc) {
-      s8 ^= (uint64_t)0xFEu << (8 * q);  // +1 (0x01) <-> -1 (0xFF)
-      dacc += dE;
-    }
+    acc = acc & in;
+    s8 ^= acc ? ((uint64_t)0xFEu << (8 * q)) : 0ull;
+    dacc += acc ? f_to_ll_rn(f_mul(x, 2.0f * kFloatEnergyQuant)) : 0ll;
   }
-  *reinterpret_cast<uint64_t*>(sp + (size_t)g * kGroup) = s8;
+  *reinterpret_cast<uint64_t*>(sp + g * kGroup) = s8;
   return dacc;
 }
 
-template <bool kInt, bool kInSmem>
+template <bool kInt, bool kInSmem, int W, bool kField>
 __global__ void __launch_bounds__(1024, 1) pt_run_kernel(const PtKernelArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const SmemLayout L = smem_layout(a.n_pos, a.rpc, a.R, a.F, a.n_colors, a.n_slices, a.n_ell, kInt, kInSmem);
+  const SmemLayout L = smem_layout(a.n_pos, a.rpc, a.R, a.F, a.n_colors, a.n_slices, a.n_ell, kInt, kInSmem,
+                                   (int)blockDim.x);
   int8_t* sp = reinterpret_cast<int8_t*>(smem + L.spins);
   long long* eacc = reinterpret_cast<long long*>(smem + L.eacc);
   long long* ecur = reinterpret_cast<long long*>(smem + L.ecur);
@@ -150,7 +217,6 @@ __global__ void __launch_bounds__(1024, 1) pt_run_kernel(const PtKernelArgs a) {
     for (int i = tid; i < nv; i += B) dst[i] = src[i];
   }
   for (int i = tid; i < nloc; i += B) {
-    eacc[i] = 0;
     ecur[i] = a.energy[s0 + i];
     ebest[i] = a.best_energy[s0 + i];
     imp[i] = 0;
@@ -164,34 +230,41 @@ __global__ void __launch_bounds__(1024, 1) pt_run_kernel(const PtKernelArgs a) {
     for (int i = tid; i < R * a.F; i += B) thr_sm[i] = a.thr[i];
   for (int i = tid; i < 2 * (R - 1); i += B) stats[i] = 0;
   for (int i = tid; i <= a.n_colors; i += B) cptr[i] = a.color_ptr[i];
-  const int* soff = a.slice_off;
-  const int* nbr = a.ell_nbr;
-  const void* wv = a.ell_w;
-  const void* hv = a.h_pos;
+  Tables T;
+  T.soff = a.slice_off;
+  T.ent = nullptr;
+  T.nbr = a.ell_nbr;
+  T.w8 = static_cast<const int8_t*>(a.ell_w);
+  T.wf = static_cast<const float*>(a.ell_w);
+  T.h = a.h_pos;
   if constexpr (kInSmem) {
     int* soff_sm = reinterpret_cast<int*>(smem + L.soff);
-    int* nbr_sm = reinterpret_cast<int*>(smem + L.nbr);
     for (int i = tid; i <= a.n_slices; i += B) soff_sm[i] = a.slice_off[i];
-    {
+    if constexpr (kInt) {
+      // pack (neighbour position, int8 weight) into one word: one shared load per coupling
+      uint32_t* ent_sm = reinterpret_cast<uint32_t*>(smem + L.nbr);
+      const int8_t* w8 = static_cast<const int8_t*>(a.ell_w);
+      for (int i = tid; i < (int)a.n_ell; i += B)
+        ent_sm[i] = (uint32_t)a.ell_nbr[i] | ((uint32_t)(uint8_t)w8[i] << 24);
+      T.ent = ent_sm;
+    } else {
+      int* nbr_sm = reinterpret_cast<int*>(smem + L.nbr);
       const int4* s4 = reinterpret_cast<const int4*>(a.ell_nbr);
       int4* d4 = reinterpret_cast<int4*>(nbr_sm);
-      for (long long i = tid; i < a.n_ell / 4; i += B) d4[i] = s4[i];
-    }
-    {
-      const long long wbytes = kInt ? a.n_ell : a.n_ell * 4;
-      const int4* s4 = reinterpret_cast<const int4*>(a.ell_w);
-      int4* d4 = reinterpret_cast<int4*>(smem + L.w);
-      for (long long i = tid; i < wbytes / 16; i += B) d4[i] = s4[i];
+      for (int i = tid; i < (int)(a.n_ell / 4); i += B) d4[i] = s4[i];
+      const int4* w4 = reinterpret_cast<const int4*>(a.ell_w);
+      int4* dw = reinterpret_cast<int4*>(smem + L.w);
+      for (int i = tid; i < (int)(a.n_ell / 4); i += B) dw[i] = w4[i];
+      T.nbr = nbr_sm;
+      T.wf = reinterpret_cast<const float*>(smem + L.w);
     }
     {
       const int4* s4 = reinterpret_cast<const int4*>(a.h_pos);
       int4* d4 = reinterpret_cast<int4*>(smem + L.h);
       for (int i = tid; i < n_pos / 4; i += B) d4[i] = s4[i];
     }
-    soff = soff_sm;
-    nbr = nbr_sm;
-    wv = smem + L.w;
-    hv = smem + L.h;
+    T.soff = soff_sm;
+    T.h = smem + L.h;
   }
   if (tid == 0) {
     ctl[0] = 0;  // abort flag
@@ -204,32 +277,47 @@ __global__ void __launch_bounds__(1024, 1) pt_run_kernel(const PtKernelArgs a) {
     for (int i = tid; i < nloc; i += B) nb_sm[i] = -2.0f * (float)beta_sm[rung_sm[s0 + i]];
   __syncthreads();
 
+  // Thread -> slot binding: `tps` consecutive threads serve one slot for the whole launch, so each
+  // thread keeps its slot's energy change in a register (no atomics in the sweep loop).
+  const int tps = B / a.rpc;
+  const int seg = seg_width(B, a.rpc);
+  const int my_sl = tid / tps, lt = tid - my_sl * tps;
+  const bool active = my_sl < nloc;
+  const int my_slot = s0 + (active ? my_sl : 0);
+  int8_t* my_sp = sp + (size_t)(active ? my_sl : 0) * n_pos;
   const int k = a.n_colors;
+  const uint32_t c_sweep = ctr3(kTagSweep, a.inst), c_second = ctr3(kTagSecond, a.inst);
   for (int j = 0; j < a.n_rounds; ++j) {
     const long long round = a.round0 + j;
+    long long dacc = 0;
+    const uint32_t* thr_rung = kInt ? thr_sm + (size_t)rung_sm[my_slot] * a.F : nullptr;
+    const float neg2beta = kInt ? 0.0f : nb_sm[active ? my_sl : 0];
     for (int sw = 0; sw < a.spr; ++sw) {
       const uint32_t t = (uint32_t)(round * a.spr + sw);
       for (int c = 0; c < k; ++c) {
         const int lo = cptr[c], hi = cptr[c + 1];
-        const int glo = lo >> 3, ghi = (hi + 7) >> 3, ng = ghi - glo;
-        const int items = nloc * ng;
-        for (int it = tid; it < items; it += B) {
-          const int sl = (nloc == 1) ? 0 : it / ng;
-          const int g = glo + (it - sl * ng);
-          const int slot = s0 + sl;
-          const long long d = sweep_group<kInt, kInSmem>(
-              g, lo, hi, t, slot, sp + (size_t)sl * n_pos, soff, nbr, wv, hv,
-              kInt ? thr_sm + (size_t)rung_sm[slot] * a.F : nullptr, a.F,
-              kInt ? 0.0f : nb_sm[sl], a.inst, a.k0, a.k1);
-          if (d != 0) atomicAdd(reinterpret_cast<unsigned long long*>(eacc + sl), (unsigned long long)d);
+        const int ghi = (hi + 7) >> 3;
+        if (active) {
+          for (int g = (lo >> 3) + lt; g < ghi; g += tps) {
+            if constexpr (kInt)
+              dacc += group_int<W, kInSmem, kField>(g, lo, hi, t, (uint32_t)my_slot, my_sp, T, thr_rung, a.F,
+                                                    c_sweep, c_second, a.k0, a.k1);
+            else
+              dacc += group_f32<W, kInSmem, kField>(g, lo, hi, t, (uint32_t)my_slot, my_sp, T, neg2beta, c_sweep,
+                                                    c_second, a.k0, a.k1);
+          }
         }
         __syncthreads();
       }
     }
-    // ---- round end: energies, per-slot best, publication ----
+    // ---- round end: reduce the energy change of each slot over its threads ----
+    for (int off = seg >> 1; off > 0; off >>= 1) dacc += __shfl_xor_sync(0xffffffffu, dacc, off);
+    if (lt % seg == 0) eacc[tid / seg] = dacc;
+    __syncthreads();
     for (int i = tid; i < nloc; i += B) {
-      const long long e = ecur[i] + eacc[i];
-      eacc[i] = 0;
+      long long e = ecur[i];
+      const int nseg = tps / seg;
+      for (int q = 0; q < nseg; ++q) e += eacc[i * nseg + q];
       ecur[i] = e;
       imp[i] = (e < ebest[i]) ? 1 : 0;
       if (e < ebest[i]) ebest[i] = e;
@@ -482,9 +570,21 @@ cudaError_t launch_energy_fp64(const PtKernelArgs& a, int integer_path, const in
   return cudaGetLastError();
 }
 
-const void* run_kernel_ptr(int integer_path, int in_smem) {
-  if (integer_path) return in_smem ? (const void*)pt_run_kernel<true, true> : (const void*)pt_run_kernel<true, false>;
-  return in_smem ? (const void*)pt_run_kernel<false, true> : (const void*)pt_run_kernel<false, false>;
+template <bool kInt, bool kInSmem, bool kField>
+static const void* pick_w(int w) {
+  // w is the largest slice width; 0 (unknown) selects the run-time loop
+  if (w >= 1 && w <= 4) return (const void*)pt_run_kernel<kInt, kInSmem, 4, kField>;
+  if (w >= 1 && w <= 8) return (const void*)pt_run_kernel<kInt, kInSmem, 8, kField>;
+  return (const void*)pt_run_kernel<kInt, kInSmem, 0, kField>;
+}
+
+const void* run_kernel_ptr(int integer_path, int in_smem, int max_width, int has_field) {
+  if (integer_path) {
+    if (in_smem) return has_field ? pick_w<true, true, true>(max_width) : pick_w<true, true, false>(max_width);
+    return has_field ? pick_w<true, false, true>(max_width) : pick_w<true, false, false>(max_width);
+  }
+  if (in_smem) return has_field ? pick_w<false, true, true>(max_width) : pick_w<false, true, false>(max_width);
+  return has_field ? pick_w<false, false, true>(max_width) : pick_w<false, false, false>(max_width);
 }
 
 }  // namespace dpt

@@ -46,12 +46,21 @@ struct SmemLayout {
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
 
 // Byte offsets of every shared-memory array; the host sizes the launch with the same function.
+// Threads are bound to replica slots: `threads / rpc` threads per slot (a power of two below 32 or
+// a multiple of 32, so shuffle segments never straddle two slots). `eacc` holds one partial energy
+// change per shuffle segment.
+__host__ __device__ inline int seg_width(int threads, int rpc) {
+  const int tps = threads / rpc;
+  return tps < 32 ? tps : 32;
+}
+
 __host__ __device__ inline SmemLayout smem_layout(int n_pos, int rpc, int R, int F, int n_colors, int n_slices,
-                                                  long long n_ell, bool integer_path, bool ell_in_smem) {
+                                                  long long n_ell, bool integer_path, bool ell_in_smem,
+                                                  int threads) {
   SmemLayout L;
   size_t o = 0;
   L.spins = o; o = align16(o + (size_t)rpc * n_pos);
-  L.eacc = o;  o = align16(o + 8 * (size_t)rpc);
+  L.eacc = o;  o = align16(o + 8 * (size_t)(threads / seg_width(threads, rpc)));
   L.ecur = o;  o = align16(o + 8 * (size_t)rpc);
   L.ebest = o; o = align16(o + 8 * (size_t)rpc);
   L.imp = o;   o = align16(o + 4 * (size_t)rpc);
@@ -67,8 +76,8 @@ __host__ __device__ inline SmemLayout smem_layout(int n_pos, int rpc, int R, int
   L.soff = L.nbr = L.w = L.h = o;
   if (ell_in_smem) {
     L.soff = o; o = align16(o + 4 * (size_t)(n_slices + 1));
-    L.nbr = o;  o = align16(o + 4 * (size_t)n_ell);
-    L.w = o;    o = align16(o + (integer_path ? 1 : 4) * (size_t)n_ell);
+    L.nbr = o;  o = align16(o + 4 * (size_t)n_ell);  // integer path: packed neighbour | weight << 24
+    L.w = o;    o = align16(o + (integer_path ? 0 : 4) * (size_t)n_ell);
     L.h = o;    o = align16(o + 4 * (size_t)n_pos);
   }
   L.total = o;
@@ -78,6 +87,6 @@ __host__ __device__ inline SmemLayout smem_layout(int n_pos, int rpc, int R, int
 cudaError_t launch_init(const PtKernelArgs& a, int integer_path, cudaStream_t st);
 cudaError_t launch_energy_fp64(const PtKernelArgs& a, int integer_path, const int8_t* spins, int R, double* out,
                                cudaStream_t st);
-const void* run_kernel_ptr(int integer_path, int in_smem);
+const void* run_kernel_ptr(int integer_path, int in_smem, int max_width, int has_field);
 
 }  // namespace dpt

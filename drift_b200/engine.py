@@ -104,7 +104,7 @@ class DeviceProblem:
 
     def c_problem(self) -> _lib.DeviceProblem:
         return _lib.DeviceProblem(self.n, self.n_pos, self.n_slices, self.info.n_colors, 1 if self.integer_path else 0,
-                                  self.max_field, self.max_width, self.max_class, 0, self.n_ell,
+                                  self.max_field, self.max_width, self.max_class, self.info.has_field, self.n_ell,
                                   self.d_color_ptr.data_ptr(), self.d_slice_off.data_ptr(), self.d_ell_nbr.data_ptr(),
                                   self.d_ell_w.data_ptr(), self.d_h_pos.data_ptr())
 

@@ -92,6 +92,7 @@ typedef struct DriftPtLayoutInfo {
   int32_t integer_couplings; /* 1 if every J_ij is an integer in [-127,127] and every h_i an
                                 integer in [-2^20, 2^20]                                    */
   int32_t max_field;         /* F = max_i (sum_j |J_ij| + |h_i|) on the integer path        */
+  int32_t has_field;         /* 1 if some h_i != 0                                          */
 } DriftPtLayoutInfo;
 
 DRIFT_PT_API int drift_pt_layout_query(const DriftPtCsr* csr, DriftPtLayoutInfo* info);
@@ -122,7 +123,7 @@ typedef struct DriftPtDeviceProblem {
   int32_t max_field;         /* F (integer path)                                            */
   int32_t max_width;         /* largest slice width                                         */
   int32_t max_class;         /* size of the largest colour class                            */
-  int32_t reserved0;
+  int32_t has_field;         /* 0 if every h_i == 0 (the field is then never read)          */
   int64_t n_ell;
   const int32_t* color_ptr;
   const int32_t* slice_off;
