@@ -19,6 +19,7 @@ EXPORTED = (
     "drift_pt_version", "drift_pt_last_error", "drift_pt_greedy_coloring", "drift_pt_color_order",
     "drift_pt_layout_query", "drift_pt_layout_fill", "drift_pt_thresholds", "drift_pt_workspace_bytes",
     "drift_pt_init", "drift_pt_run", "drift_pt_check", "drift_pt_energy_fp64", "drift_pt_solve",
+    "drift_pt_run_noalloc",
 )
 
 vp = C.c_void_p
@@ -101,6 +102,7 @@ def load():
     L.drift_pt_init.argtypes = [C.POINTER(DeviceProblem), C.POINTER(RunArgs), C.POINTER(DeviceState), vp]
     L.drift_pt_run.argtypes = [C.POINTER(DeviceProblem), C.POINTER(RunArgs), C.POINTER(DeviceState), vp,
                                C.c_size_t, vp]
+    L.drift_pt_run_noalloc.argtypes = [C.POINTER(DeviceProblem), C.POINTER(RunArgs), C.POINTER(DeviceState), vp]
     L.drift_pt_check.argtypes = [vp, vp]
     L.drift_pt_energy_fp64.argtypes = [C.POINTER(DeviceProblem), vp, C.c_int32, vp, vp]
     L.drift_pt_solve.argtypes = [C.POINTER(Csr), C.POINTER(SolveArgs), C.POINTER(SolveResult)]

@@ -181,6 +181,24 @@ DRIFT_PT_API int drift_pt_init(const DriftPtDeviceProblem* prob, const DriftPtRu
 DRIFT_PT_API int drift_pt_run(const DriftPtDeviceProblem* prob, const DriftPtRunArgs* args,
                  DriftPtDeviceState* state, void* workspace, size_t workspace_bytes, void* stream);
 
+/* drift_pt_run for callers that cannot allocate device memory (a framework already holds the
+ * device's memory in its own pool, a real-time loop may not call cudaMalloc after start-up, or a
+ * foreign-language binding only receives pointers to buffers others own). It takes no workspace:
+ * the scratch lives in an array built into the library, DRIFT_PT_NOALLOC_MAX_REPLICAS replicas
+ * at most (about 64 KiB, held on every GPU that loads the library until the process exits); more
+ * replicas return DRIFT_PT_EUNSUPPORTED. The caller still passes the problem, the state and the
+ * ladder. Nothing is allocated: no cudaMalloc, no cudaFree, no allocating library call.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress) while
+ * that device is current; make that first call before any stream capture. All calls in the
+ * process share the one array: calls that overlap on the GPU (other streams, other threads) race
+ * on it and must be serialised by the caller. A timed-out in-kernel wait is not reported by this
+ * entry point (drift_pt_check needs the workspace address); use drift_pt_run where that matters.
+ * No counterpart in the reference: its engine allocates all device memory itself
+ * (cuda/ising_pt.cu:180-195) and has no allocation-free mode. */
+#define DRIFT_PT_NOALLOC_MAX_REPLICAS 4096
+DRIFT_PT_API int drift_pt_run_noalloc(const DriftPtDeviceProblem* prob, const DriftPtRunArgs* args,
+                                      DriftPtDeviceState* state, void* stream);
+
 /* Synchronises the stream and returns DRIFT_PT_ETIMEOUT if the workspace's error flag is set. */
 DRIFT_PT_API int drift_pt_check(void* workspace, void* stream);
 
