@@ -249,10 +249,10 @@ def bench_b200(args):
     hp = HostProblem.from_model(model)
     prob = DeviceProblem(hp, device=dev)
     betas = ladder(w)
-    rounds = w["sweeps"] // w["spr"]
+    rounds = args.rounds or w["sweeps"] // w["spr"]
     eng = PtEngine(prob, betas, seed=1, sweeps_per_round=w["spr"], instance=rank)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
-    attempts_per_step = float(w["R"]) * w["sweeps"] * w["n"]
+    attempts_per_step = float(w["R"]) * rounds * w["spr"] * w["n"]
 
     def step(seed):
         eng.seed = seed
@@ -318,7 +318,8 @@ def bench_b200(args):
             "metric": "spin-flips/ns", "value": value, "unit": "flips/ns", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int8", "data": "synthetic",
-            "config": {"workload": w["desc"], "rounds": rounds, "sweeps_per_round": w["spr"],
+            "config": {"workload": w["desc"] + (f" [shortened to {rounds} rounds]" if args.rounds else ""),
+                       "rounds": rounds, "sweeps_per_round": w["spr"],
                        "attempts_per_step": attempts_per_step, "parallelism": f"replicas-only x{world}",
                        "l2": "flushed between steps (256 MiB write)",
                        "launch": {"rpc": eng.rpc or "auto", "threads": eng.threads or "auto"}},
@@ -348,6 +349,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="maxcut3reg", choices=list(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--rounds", type=int, default=0,
+                    help="override the rounds per step (profiling of a short case; the line then says so)")
     args = ap.parse_args()
     if args.impl == "reference":
         bench_reference(args)

@@ -33,7 +33,7 @@ class Csr(C.Structure):
 class LayoutInfo(C.Structure):
     _fields_ = [("n", C.c_int32), ("n_pos", C.c_int32), ("n_slices", C.c_int32), ("n_colors", C.c_int32),
                 ("n_ell", C.c_int64), ("max_degree", C.c_int32), ("integer_couplings", C.c_int32),
-                ("max_field", C.c_int32), ("has_field", C.c_int32)]
+                ("max_field", C.c_int32), ("has_field", C.c_int32), ("min_width", C.c_int32)]
 
 
 class Layout(C.Structure):
@@ -44,7 +44,8 @@ class Layout(C.Structure):
 class DeviceProblem(C.Structure):
     _fields_ = [("n", C.c_int32), ("n_pos", C.c_int32), ("n_slices", C.c_int32), ("n_colors", C.c_int32),
                 ("integer_path", C.c_int32), ("max_field", C.c_int32), ("max_width", C.c_int32),
-                ("max_class", C.c_int32), ("has_field", C.c_int32), ("n_ell", C.c_int64),
+                ("max_class", C.c_int32), ("has_field", C.c_int32), ("min_width", C.c_int32),
+                ("n_ell", C.c_int64),
                 ("color_ptr", vp), ("slice_off", vp), ("ell_nbr", vp), ("ell_w", vp), ("h_pos", vp)]
 
 
@@ -57,7 +58,7 @@ class RunArgs(C.Structure):
     _fields_ = [("n_replicas", C.c_int32), ("n_rounds", C.c_int32), ("sweeps_per_round", C.c_int32),
                 ("reserved0", C.c_int32), ("round_offset", C.c_int64), ("seed", C.c_uint64),
                 ("instance", C.c_uint32), ("replicas_per_cta", C.c_int32), ("threads_per_cta", C.c_int32),
-                ("reserved1", C.c_int32), ("betas", vp), ("thresholds", vp), ("timeout_s", C.c_double)]
+                ("positions_per_item", C.c_int32), ("betas", vp), ("thresholds", vp), ("timeout_s", C.c_double)]
 
 
 class SolveArgs(C.Structure):

@@ -15,7 +15,9 @@ using namespace dpt;
 
 namespace {
 
-constexpr size_t kWsHeader = 256;  // barrier counter (u64) at 0, error flag (i32) at 8
+// Workspace: 256-byte header (error flag, i32, at 8), then [2][R] int64 published energies and
+// [2][R] uint64 round tags; all of it is cleared at the start of every launch.
+constexpr size_t kWsHeader = 256;
 
 struct DeviceInfo {
   int sm_count = 0;
@@ -94,7 +96,7 @@ PtKernelArgs make_args(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, D
 extern "C" int drift_pt_workspace_bytes(int32_t n_replicas, size_t* bytes) {
   clear_error();
   if (n_replicas < 1 || !bytes) return set_error(DRIFT_PT_EINVAL, "workspace_bytes: invalid arguments");
-  *bytes = kWsHeader + ((2 * sizeof(long long) * (size_t)n_replicas + 255) & ~(size_t)255);
+  *bytes = kWsHeader + 2 * ((2 * sizeof(long long) * (size_t)n_replicas + 255) & ~(size_t)255);
   return DRIFT_PT_OK;
 }
 
@@ -116,7 +118,7 @@ extern "C" int drift_pt_init(const DriftPtDeviceProblem* prob, const DriftPtRunA
 namespace {
 
 struct LaunchPlan {
-  int rpc, threads, in_smem, grid;
+  int rpc, threads, in_smem, grid, p;
   size_t smem;
 };
 
@@ -130,26 +132,32 @@ int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPl
     return smem_layout(p->n_pos, rpc, R, p->max_field, p->n_colors, p->n_slices, p->n_ell, ip != 0, ell, threads)
         .total;
   };
-  // threads per slot: one per group of 8 positions of the largest colour class, as a power of
-  // two below 32 or a multiple of 32, with rpc * tps a multiple of 32 and at most 1024 (0 = none)
-  const int want = p->max_class / kGroup + 2;
+  // positions per item (8, 4 or 2; the fp32 path always uses 8)
+  int P = r->positions_per_item;
+  if (P != 0 && P != 8 && P != 4) return set_error(DRIFT_PT_EINVAL, "positions_per_item must be 0, 4 or 8");
+  if (!ip) P = 8;
+  else if (P == 0) P = 4;  // measured faster on the integer path: shorter per-item dependency chains
+  // threads per slot: one per item of the largest colour class (32-group runs times 8/P
+  // sub-blocks), as a power of two below 32 or a multiple of 32, with rpc * tps a multiple of 32
+  // and at most kMaxThreads (0 = none)
+  const int want = ((p->max_class / kGroup + 2 + 31) / 32) * 32 * (kGroup / P);
   auto pick_tps = [&](int rpc) -> int {
     int tps = 1;
     while (tps < 32 && tps < want) tps *= 2;
     if (tps >= 32) tps = ((want + 31) / 32) * 32;
-    while (rpc * tps > 1024 && tps > 1) tps = tps > 32 ? tps - 32 : tps / 2;
+    while (rpc * tps > kMaxThreads && tps > 1) tps = tps > 32 ? tps - 32 : tps / 2;
     while ((rpc * tps) % 32 != 0) {
       tps = tps < 32 ? tps * 2 : tps + 32;
-      if (rpc * tps > 1024) return 0;
+      if (rpc * tps > kMaxThreads) return 0;
     }
-    return rpc * tps <= 1024 ? tps : 0;
+    return rpc * tps <= kMaxThreads ? tps : 0;
   };
   int rpc = r->replicas_per_cta;
   if (rpc <= 0) {
     // Work of one round on one replica vs the cost of a grid-wide barrier (~5 us): small
     // problems keep every replica in one CTA and need no barrier at all.
     const double work = (double)R * p->n * std::max(1, r->sweeps_per_round);
-    if (work <= 65536.0 && R <= 1024 && pick_tps(R) > 0 && total(R, false, R * pick_tps(R)) <= (size_t)di.max_smem_optin)
+    if (work <= 65536.0 && R <= kMaxThreads && pick_tps(R) > 0 && total(R, false, R * pick_tps(R)) <= (size_t)di.max_smem_optin)
       rpc = R;
     else
       rpc = 1;
@@ -168,9 +176,9 @@ int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPl
   {
     const int tps = threads / rpc;
     const bool pow2 = tps > 0 && (tps & (tps - 1)) == 0;
-    if (threads < 32 || threads > 1024 || threads % 32 || threads % rpc || !(tps % 32 == 0 || (tps < 32 && pow2)))
+    if (threads < 32 || threads > kMaxThreads || threads % 32 || threads % rpc || !(tps % 32 == 0 || (tps < 32 && pow2)))
       return set_error(DRIFT_PT_EINVAL,
-                       "threads_per_cta (%d) must be a multiple of 32 in [32, 1024] and of replicas_per_cta (%d), "
+                       "threads_per_cta (%d) must be a multiple of 32 in [32, 512] and of replicas_per_cta (%d), "
                        "with threads/replica a power of two below 32 or a multiple of 32", threads, rpc);
   }
   if (total(rpc, false, threads) > (size_t)di.max_smem_optin)
@@ -178,11 +186,12 @@ int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPl
                      p->n_pos, di.max_smem_optin);
   const bool in_smem = total(rpc, true, threads) <= (size_t)di.max_smem_optin;
   lp->rpc = rpc;
+  lp->p = P;
   lp->threads = threads;
   lp->in_smem = in_smem ? 1 : 0;
   lp->grid = (R + rpc - 1) / rpc;
   lp->smem = total(rpc, in_smem, threads);
-  const void* fn = run_kernel_ptr(ip, lp->in_smem, p->max_width, p->has_field);
+  const void* fn = run_kernel_ptr(ip, lp->in_smem, p->max_width, p->min_width, p->has_field, lp->p);
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lp->smem);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
   int per_sm = 0;
@@ -219,13 +228,14 @@ extern "C" int drift_pt_run(const DriftPtDeviceProblem* prob, const DriftPtRunAr
   PtKernelArgs a = make_args(prob, args, state);
   a.rpc = lp.rpc;
   unsigned char* ws = static_cast<unsigned char*>(workspace);
-  a.bar = reinterpret_cast<unsigned long long*>(ws);
+  const size_t half = (2 * sizeof(long long) * (size_t)args->n_replicas + 255) & ~(size_t)255;
   a.err = reinterpret_cast<int*>(ws + 8);
   a.pub = reinterpret_cast<long long*>(ws + kWsHeader);
+  a.tags = reinterpret_cast<unsigned long long*>(ws + kWsHeader + half);
   const double to = args->timeout_s > 0 ? args->timeout_s : 10.0;
   a.timeout_ns = (long long)(to * 1e9);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  cudaError_t e = cudaMemsetAsync(ws, 0, kWsHeader, st);
+  cudaError_t e = cudaMemsetAsync(ws, 0, need, st);
   if (e != cudaSuccess) return cuda_fail(e, "workspace reset");
   cudaLaunchConfig_t cfg;
   std::memset(&cfg, 0, sizeof cfg);
@@ -239,7 +249,9 @@ extern "C" int drift_pt_run(const DriftPtDeviceProblem* prob, const DriftPtRunAr
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   void* kargs[] = {&a};
-  e = cudaLaunchKernelExC(&cfg, run_kernel_ptr(prob->integer_path, lp.in_smem, prob->max_width, prob->has_field), kargs);
+  e = cudaLaunchKernelExC(&cfg, run_kernel_ptr(prob->integer_path, lp.in_smem, prob->max_width, prob->min_width,
+                                                prob->has_field, lp.p),
+                          kargs);
   if (e != cudaSuccess) return cuda_fail(e, "pt_run_kernel launch");
   return DRIFT_PT_OK;
 }
@@ -366,6 +378,7 @@ extern "C" int drift_pt_solve(const DriftPtCsr* csr, const DriftPtSolveArgs* arg
   prob.integer_path = ip;
   prob.max_field = info.max_field;
   prob.max_width = info.max_degree;
+  prob.min_width = info.min_width;
   prob.max_class = max_class;
   prob.has_field = info.has_field;
   prob.n_ell = info.n_ell;

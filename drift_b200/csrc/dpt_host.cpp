@@ -144,7 +144,7 @@ extern "C" int drift_pt_layout_query(const DriftPtCsr* csr, DriftPtLayoutInfo* i
   info->n_slices = info->n_pos / kSlicePositions;
   info->n_colors = csr->n_colors;
   int64_t widths = 0;
-  int32_t maxdeg = 0;
+  int32_t maxdeg = 0, minw = 1 << 30;
   for (int32_t s = 0; s < info->n_slices; ++s) {
     int32_t w = 0;
     for (int32_t p = s * kSlicePositions; p < std::min(n, (s + 1) * kSlicePositions); ++p) {
@@ -153,9 +153,11 @@ extern "C" int drift_pt_layout_query(const DriftPtCsr* csr, DriftPtLayoutInfo* i
     }
     widths += w;
     maxdeg = std::max(maxdeg, w);
+    minw = std::min(minw, w);
   }
   info->n_ell = widths * kSlicePositions;
   info->max_degree = maxdeg;
+  info->min_width = minw;
   bool integer = true;
   int64_t F = 0;
   for (int32_t i = 0; i < n && integer; ++i) {

@@ -9,6 +9,8 @@ namespace dpt {
 // so one slice of the coupling table covers 256 positions.
 constexpr int kGroup = 8;
 constexpr int kSlicePositions = 256;
+// Largest CTA of the sweep kernel: 512 threads leave 128 registers per thread for the gathers.
+constexpr int kMaxThreads = 512;
 
 int set_error(int code, const char* fmt, ...);
 void clear_error();

@@ -34,6 +34,10 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
   return v;
 }
 
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
 __device__ __forceinline__ int ld_relaxed_i32(const int* p) {
   int v;
   asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -45,148 +49,217 @@ __device__ __forceinline__ int ld_relaxed_i32(const int* p) {
 // [lo, hi) are computed but never flipped. All gathers of the item are issued before the
 // acceptance tests (W bounds the slice width at compile time; W = 0 walks it at run time).
 // ---------------------------------------------------------------------------------------------
+// Shared memory is addressed through 32-bit byte offsets into the one dynamic shared array, so
+// every access compiles to a shared load/store with 32-bit address arithmetic.
+extern __shared__ __align__(16) unsigned char dpt_smem[];
+
+__device__ __forceinline__ uint32_t lds_u32(uint32_t off) { return *reinterpret_cast<const uint32_t*>(dpt_smem + off); }
+__device__ __forceinline__ int lds_s32(uint32_t off) { return *reinterpret_cast<const int*>(dpt_smem + off); }
+__device__ __forceinline__ float lds_f32(uint32_t off) { return *reinterpret_cast<const float*>(dpt_smem + off); }
+__device__ __forceinline__ int lds_s8(uint32_t off) { return (int)*reinterpret_cast<const int8_t*>(dpt_smem + off); }
+
 struct Tables {
-  const int* soff;        // slice offsets
-  const uint32_t* ent;    // shared-memory integer path: neighbour | weight << 24
-  const int* nbr;         // neighbour positions (float path, or global integer path)
-  const int8_t* w8;       // global integer path weights
-  const float* wf;        // float path weights
-  const void* h;          // field, [slice][q][lane]
+  // byte offsets in shared memory (tables staged in shared memory)
+  uint32_t soff_o, ent_o, nbr_o, wf_o, h_o;
+  // global pointers (tables read through L1/L2)
+  const int* soff;
+  const int* nbr;
+  const int8_t* w8;
+  const float* wf;
+  const void* h;
 };
 
 template <bool kInSmem>
-__device__ __forceinline__ void load_int_entry(const Tables& T, uint32_t e, int& nb, int& w) {
-  if constexpr (kInSmem) {
-    const uint32_t v = T.ent[e];
-    nb = (int)(v & 0xFFFFFFu);
-    w = ((int)v) >> 24;
-  } else {
-    nb = __ldg(T.nbr + e);
-    w = (int)__ldg(T.w8 + e);
-  }
+__device__ __forceinline__ int slice_off(const Tables& T, int S) {
+  if constexpr (kInSmem) return lds_s32(T.soff_o + 4u * (uint32_t)S);
+  else return __ldg(T.soff + S);
 }
 
-template <bool kInSmem>
-__device__ __forceinline__ int ld_int(const int* p) {
-  if constexpr (kInSmem) return *p;
-  else return __ldg(p);
+// P positions per item: sub-block b of group g covers positions 8g + P*b .. 8g + P*b + P-1. Every
+// item computes the group's whole Philox block and uses its own halves of it.
+template <int P> struct SpinWord;
+template <> struct SpinWord<8> { using T = uint64_t; };
+template <> struct SpinWord<4> { using T = uint32_t; };
+
+// Bits i of the result: position 8g + q0 + i lies in the colour range [lo, hi).
+template <int P>
+__device__ __forceinline__ uint32_t range_mask(int p0, int lo, int hi) {
+  const int a = min(max(lo - p0, 0), P), e = min(max(hi - p0, 0), P);
+  return ((1u << e) - 1u) & ~((1u << a) - 1u);
 }
 
-template <int W, bool kInSmem, bool kField>
-__device__ __forceinline__ int group_int(int g, int lo, int hi, uint32_t t, uint32_t slot, int8_t* __restrict__ sp,
-                                         const Tables& T, const uint32_t* __restrict__ thr_rung, int F,
-                                         uint32_t c_sweep, uint32_t c_second, uint32_t k0, uint32_t k1) {
-  const U4 rnd = philox(U4{(uint32_t)g, t, slot, c_sweep}, k0, k1);
-  const uint32_t words[4] = {rnd.x, rnd.y, rnd.z, rnd.w};
-  uint64_t s8 = *reinterpret_cast<const uint64_t*>(sp + g * kGroup);
-  const int S = g >> 5, lane = g & 31;
-  const int w0 = ld_int<kInSmem>(T.soff + S);
-  const int width = ld_int<kInSmem>(T.soff + S + 1) - w0;
+// Gather of the local fields of one item. W > 0 with kExactW: every slice has exactly W entries
+// per position, so all 2 * W * P shared loads are independent and issued before any use. W > 0
+// without kExactW: W bounds the width, loads beyond it are predicated off. W == 0: run-time loop.
+template <int W, bool kExactW, bool kInSmem, bool kField, int P>
+__device__ __forceinline__ void gather_int(int field[P], int S, int lane, int q0, uint32_t sp_o, const Tables& T) {
+  const int w0 = slice_off<kInSmem>(T, S);
+  const int width = kExactW ? W : slice_off<kInSmem>(T, S + 1) - w0;
   const uint32_t base = (uint32_t)w0 * kSlicePositions + lane;
-  int field[kGroup];
 #pragma unroll
-  for (int q = 0; q < kGroup; ++q)
-    field[q] = kField ? ld_int<kInSmem>(static_cast<const int*>(T.h) + S * kSlicePositions + q * 32 + lane) : 0;
-  auto step = [&](int d) {
-    int nb[kGroup], wt[kGroup];
-#pragma unroll
-    for (int q = 0; q < kGroup; ++q) load_int_entry<kInSmem>(T, base + (uint32_t)d * kSlicePositions + q * 32, nb[q], wt[q]);
-#pragma unroll
-    for (int q = 0; q < kGroup; ++q) field[q] += wt[q] * (int)sp[nb[q]];
-  };
+  for (int i = 0; i < P; ++i) {
+    const uint32_t hi_e = (uint32_t)(S * kSlicePositions + (q0 + i) * 32 + lane);
+    if constexpr (!kField) field[i] = 0;
+    else if constexpr (kInSmem) field[i] = lds_s32(T.h_o + 4u * hi_e);
+    else field[i] = __ldg(static_cast<const int*>(T.h) + hi_e);
+  }
   if constexpr (W > 0) {
+    uint32_t ev[W][P];
 #pragma unroll
     for (int d = 0; d < W; ++d)
-      if (d < width) step(d);
+#pragma unroll
+      for (int i = 0; i < P; ++i) {
+        const uint32_t e = base + (uint32_t)d * kSlicePositions + (uint32_t)(q0 + i) * 32;
+        if (kExactW || d < width) {
+          if constexpr (kInSmem) ev[d][i] = lds_u32(T.ent_o + 4u * e);
+          else ev[d][i] = (uint32_t)__ldg(T.nbr + e) | ((uint32_t)(uint8_t)__ldg(T.w8 + e) << 24);
+        } else {
+          ev[d][i] = 0u;  // neighbour 0 with weight 0
+        }
+      }
+    int sv[W][P];
+#pragma unroll
+    for (int d = 0; d < W; ++d)
+#pragma unroll
+      for (int i = 0; i < P; ++i) sv[d][i] = lds_s8(sp_o + (ev[d][i] & 0xFFFFFFu));
+#pragma unroll
+    for (int d = 0; d < W; ++d)
+#pragma unroll
+      for (int i = 0; i < P; ++i) field[i] += (((int)ev[d][i]) >> 24) * sv[d][i];
   } else {
-    for (int d = 0; d < width; ++d) step(d);
+    for (int d = 0; d < width; ++d) {
+      uint32_t ev[P];
+#pragma unroll
+      for (int i = 0; i < P; ++i) {
+        const uint32_t e = base + (uint32_t)d * kSlicePositions + (uint32_t)(q0 + i) * 32;
+        if constexpr (kInSmem) ev[i] = lds_u32(T.ent_o + 4u * e);
+        else ev[i] = (uint32_t)__ldg(T.nbr + e) | ((uint32_t)(uint8_t)__ldg(T.w8 + e) << 24);
+      }
+#pragma unroll
+      for (int i = 0; i < P; ++i) field[i] += (((int)ev[i]) >> 24) * lds_s8(sp_o + (ev[i] & 0xFFFFFFu));
+    }
   }
+}
+
+// sp_o: byte offset of the slot's spins; thr_o: byte offset of entry x = 0 of its rung's
+// extended threshold row (entries x = -F..F; x <= 0 is accepted before the lookup).
+template <int W, bool kExactW, bool kInSmem, bool kField, int P>
+__device__ __forceinline__ int group_int(int g, int b, int lo, int hi, uint32_t t, uint32_t slot, uint32_t sp_o,
+                                         const Tables& T, uint32_t thr_o, uint32_t c_sweep, uint32_t c_second,
+                                         uint32_t k0, uint32_t k1) {
+  using SW = typename SpinWord<P>::T;
+  const int q0 = P * b;
+  const int S = g >> 5, lane = g & 31;
+  int field[P];
+  gather_int<W, kExactW, kInSmem, kField, P>(field, S, lane, q0, sp_o, T);
+  const U4 rnd = philox(U4{(uint32_t)g, t, slot, c_sweep}, k0, k1);
+  const uint32_t words[4] = {rnd.x, rnd.y, rnd.z, rnd.w};
+  const uint32_t own_o = sp_o + (uint32_t)(g * kGroup + q0);
+  uint64_t s8 = (uint64_t)*reinterpret_cast<const SW*>(dpt_smem + own_o);
+  const uint32_t inmask = range_mask<P>(g * kGroup + q0, lo, hi);
   int dacc = 0;
 #pragma unroll
-  for (int q = 0; q < kGroup; ++q) {
-    const int p = g * kGroup + q;
-    const int si = (int)(int8_t)(uint8_t)(s8 >> (8 * q));
-    const int x = si * field[q];
-    const bool in = (p >= lo) & (p < hi);
-    const uint32_t thr = thr_rung[min(max(x, 1), F) - 1];
-    const uint32_t prim = (words[q >> 1] >> ((q & 1) * 16)) & 0xFFFFu;
+  for (int i = 0; i < P; ++i) {
+    const int q = q0 + i;
+    const int si = (int)(int8_t)(uint8_t)(s8 >> (8 * i));
+    const int x = si * field[i];
+    const uint32_t thr = lds_u32(thr_o + 4u * (uint32_t)x);
+    const uint32_t word = (P == 8) ? words[i >> 1] : (b ? words[2 + (i >> 1)] : words[i >> 1]);
+    const uint32_t prim = (word >> ((i & 1) * 16)) & 0xFFFFu;
     const uint32_t th = thr >> 16;
+    const bool in = (inmask >> i) & 1u;
     bool acc = (x <= 0) | (prim < th);
     if (in & (x > 0) & (prim == th)) {  // the first 16 bits tie: draw the second half of this uniform
-      const U4 r2 = philox(U4{(uint32_t)p, t, slot, c_second}, k0, k1);
+      const U4 r2 = philox(U4{(uint32_t)(g * kGroup + q), t, slot, c_second}, k0, k1);
       acc = (r2.x & 0xFFFFu) < (thr & 0xFFFFu);
     }
     acc = acc & in;
-    s8 ^= acc ? ((uint64_t)0xFEu << (8 * q)) : 0ull;  // +1 (0x01) <-> -1 (0xFF)
+    s8 ^= acc ? ((uint64_t)0xFEu << (8 * i)) : 0ull;  // +1 (0x01) <-> -1 (0xFF)
     dacc += acc ? 2 * x : 0;
   }
-  *reinterpret_cast<uint64_t*>(sp + g * kGroup) = s8;
+  *reinterpret_cast<SW*>(dpt_smem + own_o) = (SW)s8;
   return dacc;
 }
 
-template <int W, bool kInSmem, bool kField>
-__device__ __forceinline__ long long group_f32(int g, int lo, int hi, uint32_t t, uint32_t slot,
-                                               int8_t* __restrict__ sp, const Tables& T, float neg2beta,
-                                               uint32_t c_sweep, uint32_t c_second, uint32_t k0, uint32_t k1) {
-  const U4 rnd = philox(U4{(uint32_t)g, t, slot, c_sweep}, k0, k1);
-  const uint32_t words[4] = {rnd.x, rnd.y, rnd.z, rnd.w};
-  uint64_t s8 = *reinterpret_cast<const uint64_t*>(sp + g * kGroup);
-  const int S = g >> 5, lane = g & 31;
-  const int w0 = ld_int<kInSmem>(T.soff + S);
-  const int width = ld_int<kInSmem>(T.soff + S + 1) - w0;
+template <int W, bool kExactW, bool kInSmem, bool kField>
+__device__ __forceinline__ void gather_f32(float field[kGroup], int S, int lane, uint32_t sp_o, const Tables& T) {
+  const int w0 = slice_off<kInSmem>(T, S);
+  const int width = kExactW ? W : slice_off<kInSmem>(T, S + 1) - w0;
   const uint32_t base = (uint32_t)w0 * kSlicePositions + lane;
-  float field[kGroup];
 #pragma unroll
   for (int q = 0; q < kGroup; ++q) {
-    const float* hp = static_cast<const float*>(T.h) + S * kSlicePositions + q * 32 + lane;
-    field[q] = kField ? (kInSmem ? *hp : __ldg(hp)) : 0.0f;
+    const uint32_t hi_e = (uint32_t)(S * kSlicePositions + q * 32 + lane);
+    if constexpr (!kField) field[q] = 0.0f;
+    else if constexpr (kInSmem) field[q] = lds_f32(T.h_o + 4u * hi_e);
+    else field[q] = __ldg(static_cast<const float*>(T.h) + hi_e);
   }
+  // the sum runs over d in order (the fp32 rounding sequence is part of the definition)
   auto step = [&](int d) {
     int nb[kGroup];
     float wt[kGroup];
 #pragma unroll
     for (int q = 0; q < kGroup; ++q) {
       const uint32_t e = base + (uint32_t)d * kSlicePositions + q * 32;
-      nb[q] = ld_int<kInSmem>(T.nbr + e);
-      wt[q] = kInSmem ? T.wf[e] : __ldg(T.wf + e);
+      if constexpr (kInSmem) {
+        nb[q] = lds_s32(T.nbr_o + 4u * e);
+        wt[q] = lds_f32(T.wf_o + 4u * e);
+      } else {
+        nb[q] = __ldg(T.nbr + e);
+        wt[q] = __ldg(T.wf + e);
+      }
     }
 #pragma unroll
-    for (int q = 0; q < kGroup; ++q) field[q] = f_add(field[q], sp[nb[q]] > 0 ? wt[q] : -wt[q]);
+    for (int q = 0; q < kGroup; ++q) field[q] = f_add(field[q], lds_s8(sp_o + (uint32_t)nb[q]) > 0 ? wt[q] : -wt[q]);
   };
   if constexpr (W > 0) {
 #pragma unroll
     for (int d = 0; d < W; ++d)
-      if (d < width) step(d);
+      if (kExactW || d < width) step(d);
   } else {
     for (int d = 0; d < width; ++d) step(d);
   }
+}
+
+template <int W, bool kExactW, bool kInSmem, bool kField>
+__device__ __forceinline__ long long group_f32(int g, int lo, int hi, uint32_t t, uint32_t slot, uint32_t sp_o,
+                                               const Tables& T, float neg2beta, uint32_t c_sweep,
+                                               uint32_t c_second, uint32_t k0, uint32_t k1) {
+  const int S = g >> 5, lane = g & 31;
+  float field[kGroup];
+  gather_f32<W, kExactW, kInSmem, kField>(field, S, lane, sp_o, T);
+  const U4 rnd = philox(U4{(uint32_t)g, t, slot, c_sweep}, k0, k1);
+  const uint32_t words[4] = {rnd.x, rnd.y, rnd.z, rnd.w};
+  const uint32_t own_o = sp_o + (uint32_t)(g * kGroup);
+  uint64_t s8 = *reinterpret_cast<const uint64_t*>(dpt_smem + own_o);
+  const uint32_t inmask = range_mask<kGroup>(g * kGroup, lo, hi);
   long long dacc = 0;
 #pragma unroll
   for (int q = 0; q < kGroup; ++q) {
-    const int p = g * kGroup + q;
     const int si = (int)(int8_t)(uint8_t)(s8 >> (8 * q));
     const float x = si > 0 ? field[q] : -field[q];
-    const bool in = (p >= lo) & (p < hi);
+    const bool in = (inmask >> q) & 1u;
     const bool pos = x > 0.0f;
     const uint32_t thr = threshold_f(neg2beta, pos ? x : 0.0f);
     const uint32_t prim = (words[q >> 1] >> ((q & 1) * 16)) & 0xFFFFu;
     const uint32_t th = thr >> 16;
     bool acc = (!pos) | (prim < th);
     if (in & pos & (prim == th)) {
-      const U4 r2 = philox(U4{(uint32_t)p, t, slot, c_second}, k0, k1);
+      const U4 r2 = philox(U4{(uint32_t)(g * kGroup + q), t, slot, c_second}, k0, k1);
       acc = (r2.x & 0xFFFFu) < (thr & 0xFFFFu);
     }
     acc = acc & in;
     s8 ^= acc ? ((uint64_t)0xFEu << (8 * q)) : 0ull;
     dacc += acc ? f_to_ll_rn(f_mul(x, 2.0f * kFloatEnergyQuant)) : 0ll;
   }
-  *reinterpret_cast<uint64_t*>(sp + g * kGroup) = s8;
+  *reinterpret_cast<uint64_t*>(dpt_smem + own_o) = s8;
   return dacc;
 }
 
-template <bool kInt, bool kInSmem, int W, bool kField>
-__global__ void __launch_bounds__(1024, 1) pt_run_kernel(const PtKernelArgs a) {
-  extern __shared__ __align__(16) unsigned char smem[];
+template <bool kInt, bool kInSmem, int W, bool kExactW, bool kField, int P>
+__global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelArgs a) {
+  static_assert(P == 8 || (kInt && P == 4), "positions per item");
+  constexpr int NB = kGroup / P;  // items per group
+  unsigned char* smem = dpt_smem;
   const SmemLayout L = smem_layout(a.n_pos, a.rpc, a.R, a.F, a.n_colors, a.n_slices, a.n_ell, kInt, kInSmem,
                                    (int)blockDim.x);
   int8_t* sp = reinterpret_cast<int8_t*>(smem + L.spins);
@@ -226,13 +299,22 @@ __global__ void __launch_bounds__(1024, 1) pt_run_kernel(const PtKernelArgs a) {
     slot_sm[i] = a.slot_of_rung[i];
     beta_sm[i] = a.betas[i];
   }
-  if constexpr (kInt)
-    for (int i = tid; i < R * a.F; i += B) thr_sm[i] = a.thr[i];
+  if constexpr (kInt) {
+    // extended rows: entry x + F for x = -F..F; x <= 0 never reads its entry (always accepted)
+    const int row = 2 * a.F + 1;
+    for (int i = tid; i < R * row; i += B) {
+      const int r = i / row, x = i - r * row - a.F;
+      thr_sm[i] = x >= 1 ? a.thr[r * a.F + x - 1] : 0xFFFFFFFFu;
+    }
+  }
   for (int i = tid; i < 2 * (R - 1); i += B) stats[i] = 0;
   for (int i = tid; i <= a.n_colors; i += B) cptr[i] = a.color_ptr[i];
   Tables T;
+  T.soff_o = (uint32_t)L.soff;
+  T.ent_o = T.nbr_o = (uint32_t)L.nbr;
+  T.wf_o = (uint32_t)L.w;
+  T.h_o = (uint32_t)L.h;
   T.soff = a.slice_off;
-  T.ent = nullptr;
   T.nbr = a.ell_nbr;
   T.w8 = static_cast<const int8_t*>(a.ell_w);
   T.wf = static_cast<const float*>(a.ell_w);
@@ -246,25 +328,19 @@ __global__ void __launch_bounds__(1024, 1) pt_run_kernel(const PtKernelArgs a) {
       const int8_t* w8 = static_cast<const int8_t*>(a.ell_w);
       for (int i = tid; i < (int)a.n_ell; i += B)
         ent_sm[i] = (uint32_t)a.ell_nbr[i] | ((uint32_t)(uint8_t)w8[i] << 24);
-      T.ent = ent_sm;
     } else {
-      int* nbr_sm = reinterpret_cast<int*>(smem + L.nbr);
       const int4* s4 = reinterpret_cast<const int4*>(a.ell_nbr);
-      int4* d4 = reinterpret_cast<int4*>(nbr_sm);
+      int4* d4 = reinterpret_cast<int4*>(smem + L.nbr);
       for (int i = tid; i < (int)(a.n_ell / 4); i += B) d4[i] = s4[i];
       const int4* w4 = reinterpret_cast<const int4*>(a.ell_w);
       int4* dw = reinterpret_cast<int4*>(smem + L.w);
       for (int i = tid; i < (int)(a.n_ell / 4); i += B) dw[i] = w4[i];
-      T.nbr = nbr_sm;
-      T.wf = reinterpret_cast<const float*>(smem + L.w);
     }
     {
       const int4* s4 = reinterpret_cast<const int4*>(a.h_pos);
       int4* d4 = reinterpret_cast<int4*>(smem + L.h);
       for (int i = tid; i < n_pos / 4; i += B) d4[i] = s4[i];
     }
-    T.soff = soff_sm;
-    T.h = smem + L.h;
   }
   if (tid == 0) {
     ctl[0] = 0;  // abort flag
@@ -284,27 +360,33 @@ __global__ void __launch_bounds__(1024, 1) pt_run_kernel(const PtKernelArgs a) {
   const int my_sl = tid / tps, lt = tid - my_sl * tps;
   const bool active = my_sl < nloc;
   const int my_slot = s0 + (active ? my_sl : 0);
-  int8_t* my_sp = sp + (size_t)(active ? my_sl : 0) * n_pos;
+  const uint32_t my_sp_o = (uint32_t)L.spins + (uint32_t)(active ? my_sl : 0) * (uint32_t)n_pos;
   const int k = a.n_colors;
   const uint32_t c_sweep = ctr3(kTagSweep, a.inst), c_second = ctr3(kTagSecond, a.inst);
   for (int j = 0; j < a.n_rounds; ++j) {
     const long long round = a.round0 + j;
     long long dacc = 0;
-    const uint32_t* thr_rung = kInt ? thr_sm + (size_t)rung_sm[my_slot] * a.F : nullptr;
+    const uint32_t thr_o = kInt ? (uint32_t)L.thr + 4u * (uint32_t)(rung_sm[my_slot] * (2 * a.F + 1) + a.F) : 0u;
     const float neg2beta = kInt ? 0.0f : nb_sm[active ? my_sl : 0];
     for (int sw = 0; sw < a.spr; ++sw) {
       const uint32_t t = (uint32_t)(round * a.spr + sw);
       for (int c = 0; c < k; ++c) {
         const int lo = cptr[c], hi = cptr[c + 1];
-        const int ghi = (hi + 7) >> 3;
+        const int glo = lo >> 3, ghi = (hi + 7) >> 3;
+        // item v -> (group, sub-block): 32 consecutive items are 32 consecutive groups (coalesced
+        // coupling reads), the NB sub-blocks of those groups follow as the next 32-item runs
+        const int span = ((ghi - glo + 31) >> 5) * 32 * NB;
         if (active) {
-          for (int g = (lo >> 3) + lt; g < ghi; g += tps) {
+          for (int v = lt; v < span; v += tps) {
+            const int b = (v >> 5) & (NB - 1);
+            const int g = glo + (v / (32 * NB)) * 32 + (v & 31);
+            if (g >= ghi) continue;
             if constexpr (kInt)
-              dacc += group_int<W, kInSmem, kField>(g, lo, hi, t, (uint32_t)my_slot, my_sp, T, thr_rung, a.F,
-                                                    c_sweep, c_second, a.k0, a.k1);
+              dacc += group_int<W, kExactW, kInSmem, kField, P>(g, b, lo, hi, t, (uint32_t)my_slot, my_sp_o, T,
+                                                                thr_o, c_sweep, c_second, a.k0, a.k1);
             else
-              dacc += group_f32<W, kInSmem, kField>(g, lo, hi, t, (uint32_t)my_slot, my_sp, T, neg2beta, c_sweep,
-                                                    c_second, a.k0, a.k1);
+              dacc += group_f32<W, kExactW, kInSmem, kField>(g, lo, hi, t, (uint32_t)my_slot, my_sp_o, T, neg2beta,
+                                                             c_sweep, c_second, a.k0, a.k1);
           }
         }
         __syncthreads();
@@ -321,35 +403,45 @@ __global__ void __launch_bounds__(1024, 1) pt_run_kernel(const PtKernelArgs a) {
       ecur[i] = e;
       imp[i] = (e < ebest[i]) ? 1 : 0;
       if (e < ebest[i]) ebest[i] = e;
-      if (gridDim.x > 1) __stcg(a.pub + (size_t)(round & 1) * R + s0 + i, e);
+      if (gridDim.x > 1) {
+        // publish: the energy, then (release-ordered after it) the round tag that readers poll
+        const size_t at = (size_t)(round & 1) * R + s0 + i;
+        __stcg(a.pub + at, e);
+        st_release_u64(a.tags + at, (unsigned long long)round + 1ull);
+      }
     }
     __syncthreads();
-    for (int sl = 0; sl < nloc; ++sl) {
-      if (!imp[sl]) continue;  // uniform across the block
-      const int4* src = reinterpret_cast<const int4*>(sp + (size_t)sl * n_pos);
-      int4* dst = reinterpret_cast<int4*>(a.best_spins + (size_t)(s0 + sl) * n_pos);
-      for (int i = tid; i < n_pos / 16; i += B) dst[i] = src[i];
+    {
+      // copy the spins of every slot that reached a new best, all slots in one pass
+      const int chunks = n_pos / 16;
+      const int4* src = reinterpret_cast<const int4*>(sp);
+      int4* dst = reinterpret_cast<int4*>(a.best_spins + (size_t)s0 * n_pos);
+      for (int i = tid; i < nloc * chunks; i += B)
+        if (imp[i / chunks]) dst[i] = src[i];
     }
     if (gridDim.x > 1) {
-      if (tid == 0) {
-        __threadfence();
-        atomicAdd(a.bar, 1ULL);
-        const unsigned long long target = (unsigned long long)(j + 1) * gridDim.x;
-        const unsigned long long t0 = global_timer_ns();
-        int abort_now = 0;
-        while (ld_acquire_u64(a.bar) < target) {
-          if (ld_relaxed_i32(a.err) != 0) { abort_now = 1; break; }
-          if (global_timer_ns() - t0 > (unsigned long long)a.timeout_ns) {
-            atomicExch(a.err, DRIFT_PT_ETIMEOUT);
-            abort_now = 1;
-            break;
+      // gather every slot's energy of this round: poll its tag (acquire), then read the energy;
+      // this is the only grid-wide synchronisation of the round, bounded by the timeout
+      int abort_now = 0;
+      const unsigned long long want = (unsigned long long)round + 1ull;
+      for (int s = tid; s < R && !abort_now; s += B) {
+        const size_t at = (size_t)(round & 1) * R + s;
+        if (ld_acquire_u64(a.tags + at) < want) {
+          const unsigned long long t0 = global_timer_ns();
+          while (ld_acquire_u64(a.tags + at) < want) {
+            if (ld_relaxed_i32(a.err) != 0) { abort_now = 1; break; }
+            if (global_timer_ns() - t0 > (unsigned long long)a.timeout_ns) {
+              atomicExch(a.err, DRIFT_PT_ETIMEOUT);
+              abort_now = 1;
+              break;
+            }
           }
         }
-        ctl[0] = abort_now;
+        if (!abort_now) eall[s] = __ldcg(a.pub + at);
       }
+      if (abort_now) ctl[0] = 1;
       __syncthreads();
       if (ctl[0]) break;
-      for (int i = tid; i < R; i += B) eall[i] = __ldcg(a.pub + (size_t)(round & 1) * R + i);
     } else {
       for (int i = tid; i < R; i += B) eall[i] = ecur[i];
     }
@@ -570,21 +662,36 @@ cudaError_t launch_energy_fp64(const PtKernelArgs& a, int integer_path, const in
   return cudaGetLastError();
 }
 
-template <bool kInt, bool kInSmem, bool kField>
-static const void* pick_w(int w) {
-  // w is the largest slice width; 0 (unknown) selects the run-time loop
-  if (w >= 1 && w <= 4) return (const void*)pt_run_kernel<kInt, kInSmem, 4, kField>;
-  if (w >= 1 && w <= 8) return (const void*)pt_run_kernel<kInt, kInSmem, 8, kField>;
-  return (const void*)pt_run_kernel<kInt, kInSmem, 0, kField>;
+template <bool kInt, bool kInSmem, bool kField, int P>
+static const void* pick_w(int max_w, int min_w) {
+  // uniform slice widths 3, 4 and 6 (regular graphs and lattices) get an exact-width gather;
+  // otherwise widths up to 8 a predicated one, and wider slices a run-time loop
+  if constexpr (kInSmem) {
+    if (min_w == max_w && max_w == 3) return (const void*)pt_run_kernel<kInt, kInSmem, 3, true, kField, P>;
+    if (min_w == max_w && max_w == 4) return (const void*)pt_run_kernel<kInt, kInSmem, 4, true, kField, P>;
+    if (min_w == max_w && max_w == 6) return (const void*)pt_run_kernel<kInt, kInSmem, 6, true, kField, P>;
+  }
+  if (max_w >= 1 && max_w <= 8) return (const void*)pt_run_kernel<kInt, kInSmem, 8, false, kField, P>;
+  return (const void*)pt_run_kernel<kInt, kInSmem, 0, false, kField, P>;
 }
 
-const void* run_kernel_ptr(int integer_path, int in_smem, int max_width, int has_field) {
-  if (integer_path) {
-    if (in_smem) return has_field ? pick_w<true, true, true>(max_width) : pick_w<true, true, false>(max_width);
-    return has_field ? pick_w<true, false, true>(max_width) : pick_w<true, false, false>(max_width);
+template <bool kInt, bool kInSmem, bool kField>
+static const void* pick_p(int max_w, int min_w, int p) {
+  if constexpr (kInt) {
+    if (p == 4) return pick_w<kInt, kInSmem, kField, 4>(max_w, min_w);
   }
-  if (in_smem) return has_field ? pick_w<false, true, true>(max_width) : pick_w<false, true, false>(max_width);
-  return has_field ? pick_w<false, false, true>(max_width) : pick_w<false, false, false>(max_width);
+  return pick_w<kInt, kInSmem, kField, 8>(max_w, min_w);
+}
+
+const void* run_kernel_ptr(int integer_path, int in_smem, int max_width, int min_width, int has_field,
+                           int positions_per_item) {
+  const int p = positions_per_item, w = max_width, m = min_width;
+  if (integer_path) {
+    if (in_smem) return has_field ? pick_p<true, true, true>(w, m, p) : pick_p<true, true, false>(w, m, p);
+    return has_field ? pick_p<true, false, true>(w, m, p) : pick_p<true, false, false>(w, m, p);
+  }
+  if (in_smem) return has_field ? pick_p<false, true, true>(w, m, p) : pick_p<false, true, false>(w, m, p);
+  return has_field ? pick_p<false, false, true>(w, m, p) : pick_p<false, false, false>(w, m, p);
 }
 
 }  // namespace dpt

@@ -32,9 +32,9 @@ struct PtKernelArgs {
   long long* accepted;
   double* best_hist;
   // workspace
-  unsigned long long* bar;
   int* err;
-  long long* pub;
+  long long* pub;                // [2][R] energies published per round parity
+  unsigned long long* tags;      // [2][R] round + 1 once the matching energy is visible
   long long timeout_ns;
 };
 
@@ -69,7 +69,7 @@ __host__ __device__ inline SmemLayout smem_layout(int n_pos, int rpc, int R, int
   L.slot = o;  o = align16(o + 4 * (size_t)R);
   L.beta = o;  o = align16(o + 8 * (size_t)R);
   L.nb = o;    o = align16(o + 4 * (size_t)rpc);
-  L.thr = o;   o = align16(o + (integer_path ? 4 * (size_t)R * F : 0));
+  L.thr = o;   o = align16(o + (integer_path ? 4 * (size_t)R * (2 * F + 1) : 0));  // rows for x = -F..F
   L.stats = o; o = align16(o + 8 * (size_t)(R > 1 ? R - 1 : 0));
   L.cptr = o;  o = align16(o + 4 * (size_t)(n_colors + 1));
   L.ctl = o;   o = align16(o + 16);
@@ -87,6 +87,7 @@ __host__ __device__ inline SmemLayout smem_layout(int n_pos, int rpc, int R, int
 cudaError_t launch_init(const PtKernelArgs& a, int integer_path, cudaStream_t st);
 cudaError_t launch_energy_fp64(const PtKernelArgs& a, int integer_path, const int8_t* spins, int R, double* out,
                                cudaStream_t st);
-const void* run_kernel_ptr(int integer_path, int in_smem, int max_width, int has_field);
+const void* run_kernel_ptr(int integer_path, int in_smem, int max_width, int min_width, int has_field,
+                           int positions_per_item);
 
 }  // namespace dpt

@@ -1,14 +1,14 @@
 // dpt_noalloc.cu - drift_pt_run_noalloc: the PT round loop without any device allocation.
 //
-// drift_pt_run needs a scratch workspace (grid-barrier counter, error flag, per-round energy
-// publication buffer) that the caller allocates. Some callers cannot allocate device memory at
+// drift_pt_run needs a scratch workspace (error flag, per-round energy publication buffer and
+// its round tags, which are also the grid-wide synchronisation) that the caller allocates. Some callers cannot allocate device memory at
 // all: code that runs after a framework has reserved the device's memory for its own pool, hosts
 // whose allocation policy forbids cudaMalloc outside start-up (real-time or embedded loops), and
 // foreign-language bindings that only receive pointers to buffers someone else owns. For them
 // this entry point uses a scratch array compiled into the library instead.
 //
 // The scratch array is a file-scope __device__ variable, so every GPU that loads the library holds
-// kNoAllocBytes (about 64 KiB) of it until the process exits. On the host its name is only a
+// kNoAllocBytes (about 128 KiB) of it until the process exits. On the host its name is only a
 // stand-in symbol, never a device address: the device address is looked up once per device with
 // cudaGetSymbolAddress (on the first call made while that device is current) and cached.
 #include <cuda_runtime.h>
@@ -21,8 +21,8 @@
 
 namespace {
 
-// drift_pt_workspace_bytes(DRIFT_PT_NOALLOC_MAX_REPLICAS): 256-byte header + 16 bytes per replica
-constexpr size_t kNoAllocBytes = 256 + 16 * (size_t)DRIFT_PT_NOALLOC_MAX_REPLICAS;
+// drift_pt_workspace_bytes(DRIFT_PT_NOALLOC_MAX_REPLICAS): 256-byte header + 32 bytes per replica
+constexpr size_t kNoAllocBytes = 256 + 32 * (size_t)DRIFT_PT_NOALLOC_MAX_REPLICAS;
 
 std::mutex g_mu;
 std::vector<void*> g_scratch_addr;  // device address of the scratch array, per device ordinal
@@ -62,7 +62,7 @@ extern "C" int drift_pt_run_noalloc(const DriftPtDeviceProblem* prob, const Drif
     }
     scratch = g_scratch_addr[dev];
   }
-  // drift_pt_run clears the barrier counter and error flag at the start of every launch, so the
-  // contents left by the previous call do not matter.
+  // drift_pt_run clears the whole scratch (error flag, published energies, round tags) at the
+  // start of every launch, so the contents left by the previous call do not matter.
   return drift_pt_run(prob, args, state, scratch, kNoAllocBytes, stream);
 }

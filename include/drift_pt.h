@@ -93,6 +93,7 @@ typedef struct DriftPtLayoutInfo {
                                 integer in [-2^20, 2^20]                                    */
   int32_t max_field;         /* F = max_i (sum_j |J_ij| + |h_i|) on the integer path        */
   int32_t has_field;         /* 1 if some h_i != 0                                          */
+  int32_t min_width;         /* smallest slice width (== max_degree: uniform, e.g. lattices) */
 } DriftPtLayoutInfo;
 
 DRIFT_PT_API int drift_pt_layout_query(const DriftPtCsr* csr, DriftPtLayoutInfo* info);
@@ -124,6 +125,8 @@ typedef struct DriftPtDeviceProblem {
   int32_t max_width;         /* largest slice width                                         */
   int32_t max_class;         /* size of the largest colour class                            */
   int32_t has_field;         /* 0 if every h_i == 0 (the field is then never read)          */
+  int32_t min_width;         /* smallest slice width; the layout's values of max_field,
+                                max_width and min_width must be passed unchanged            */
   int64_t n_ell;
   const int32_t* color_ptr;
   const int32_t* slice_off;
@@ -158,8 +161,8 @@ typedef struct DriftPtRunArgs {
   uint64_t seed;
   uint32_t instance;         /* stream id (< 2^24), distinct per independent chain set      */
   int32_t replicas_per_cta;  /* 0 = auto (autotuner)                                        */
-  int32_t threads_per_cta;   /* 0 = auto                                                    */
-  int32_t reserved1;
+  int32_t threads_per_cta;   /* 0 = auto; at most 512                                       */
+  int32_t positions_per_item;/* 8 or 4 spins per thread and phase (integer path); 0 = auto  */
   const double* betas;       /* [R] inverse temperature of each rung                        */
   const uint32_t* thresholds;/* [R][F] integer path (from drift_pt_thresholds), else NULL   */
   double timeout_s;          /* bound on any in-kernel wait (0 = 10 s)                      */
@@ -185,7 +188,7 @@ DRIFT_PT_API int drift_pt_run(const DriftPtDeviceProblem* prob, const DriftPtRun
  * device's memory in its own pool, a real-time loop may not call cudaMalloc after start-up, or a
  * foreign-language binding only receives pointers to buffers others own). It takes no workspace:
  * the scratch lives in an array built into the library, DRIFT_PT_NOALLOC_MAX_REPLICAS replicas
- * at most (about 64 KiB, held on every GPU that loads the library until the process exits); more
+ * at most (about 128 KiB, held on every GPU that loads the library until the process exits); more
  * replicas return DRIFT_PT_EUNSUPPORTED. The caller still passes the problem, the state and the
  * ladder. Nothing is allocated: no cudaMalloc, no cudaFree, no allocating library call.
  * The first call on a device looks up the array's device address (cudaGetSymbolAddress) while

@@ -30,13 +30,14 @@ def oracle_problem(hp: HostProblem, integer_path: bool):
                                 integer_path=integer_path)
 
 
-def run_engine(model, betas, rounds, spr, seed, *, rpc=0, threads=0, instance=0, chunks=None, integer_path=None):
+def run_engine(model, betas, rounds, spr, seed, *, rpc=0, threads=0, ppi=0, instance=0, chunks=None,
+               integer_path=None):
     import torch
 
     hp = HostProblem.from_model(model)
     prob = DeviceProblem(hp, integer_path=integer_path)
     eng = PtEngine(prob, betas, seed=seed, sweeps_per_round=spr, instance=instance, replicas_per_cta=rpc,
-                   threads_per_cta=threads)
+                   threads_per_cta=threads, positions_per_item=ppi)
     eng.init()
     hist = torch.zeros(max(rounds, 1), dtype=torch.float64, device="cuda")
     done = 0
@@ -84,12 +85,13 @@ def test_engine_matches_oracle_bit_exact(name):
     assert_bit_exact(st, ost, hist, rounds)
 
 
-@pytest.mark.parametrize("rpc,threads", [(1, 64), (1, 1024), (2, 256), (8, 512), (64, 1024)])
-def test_results_do_not_depend_on_launch_shape(rpc, threads):
+@pytest.mark.parametrize("rpc,threads,ppi", [(1, 64, 8), (1, 512, 8), (2, 256, 8), (8, 512, 8), (64, 512, 8),
+                                              (1, 0, 4), (1, 96, 4), (4, 512, 4), (64, 512, 4), (16, 0, 0)])
+def test_results_do_not_depend_on_launch_shape(rpc, threads, ppi):
     model = maxcut_3regular(2048, 5)
     R, rounds, spr, seed = 64, 10, 2, 11
     betas = geometric_betas(R, 0.25, 5.0)
-    hp, prob, eng, st, hist = run_engine(model, betas, rounds, spr, seed, rpc=rpc, threads=threads)
+    hp, prob, eng, st, hist = run_engine(model, betas, rounds, spr, seed, rpc=rpc, threads=threads, ppi=ppi)
     ost = oracle.pt_run(oracle_problem(hp, True), betas, n_rounds=rounds, sweeps_per_round=spr, seed=seed, thr=eng.thr)
     assert_bit_exact(st, ost, hist, rounds)
 
@@ -113,6 +115,25 @@ def test_resume_equals_single_run_integer():
     ost = oracle.pt_run(oracle_problem(hp, True), betas, n_rounds=sum(chunks), sweeps_per_round=spr, seed=seed,
                         thr=eng.thr)
     assert_bit_exact(st, ost, hist, sum(chunks))
+
+
+@pytest.mark.parametrize("ppi", [8, 4])
+def test_integer_field_and_wide_slices_small_items(ppi):
+    # integer couplings with an integer field (kField) and degree-6 slices (W = 8) on short items
+    from drift_b200.instances import ea_3d
+    from drift_b200.ising import SparseIsingModel
+
+    base = ea_3d(8, 2)
+    rp, ci, w = base.csr()
+    rows = np.repeat(np.arange(base.n), np.diff(rp))
+    up = rows < ci
+    rng = np.random.default_rng(1)
+    model = SparseIsingModel(base.n, rows[up], ci[up], w[up], rng.integers(-2, 3, size=base.n).astype(float))
+    betas = geometric_betas(12, 0.3, 3.0)
+    hp, prob, eng, st, hist = run_engine(model, betas, 20, 3, 6, ppi=ppi)
+    assert prob.integer_path and prob.info.has_field
+    ost = oracle.pt_run(oracle_problem(hp, True), betas, n_rounds=20, sweeps_per_round=3, seed=6, thr=eng.thr)
+    assert_bit_exact(st, ost, hist, 20)
 
 
 def test_integer_couplings_forced_onto_fp32_path_match_oracle():
