@@ -19,7 +19,8 @@ EXPORTED = (
     "drift_pt_version", "drift_pt_last_error", "drift_pt_greedy_coloring", "drift_pt_color_order",
     "drift_pt_layout_query", "drift_pt_layout_fill", "drift_pt_thresholds", "drift_pt_workspace_bytes",
     "drift_pt_init", "drift_pt_run", "drift_pt_check", "drift_pt_energy_fp64", "drift_pt_solve",
-    "drift_pt_run_noalloc",
+    "drift_pt_run_noalloc", "drift_pt_batch_items", "drift_pt_batch_init", "drift_pt_batch_workspace_bytes",
+    "drift_pt_batch_run",
 )
 
 vp = C.c_void_p
@@ -73,6 +74,21 @@ class SolveResult(C.Structure):
                 ("swap_tried", vp), ("swap_accepted", vp), ("best_history", vp)]
 
 
+class BatchProblem(C.Structure):
+    _fields_ = [("n_instances", C.c_int32), ("integer_path", C.c_int32), ("has_field", C.c_int32),
+                ("max_width", C.c_int32), ("min_width", C.c_int32), ("max_field", C.c_int32),
+                ("max_n_pos", C.c_int32), ("max_colors", C.c_int32), ("total_slots", C.c_int64),
+                ("desc", vp), ("color_ptr", vp), ("slice_off", vp), ("ell_nbr", vp), ("ell_w", vp), ("h_pos", vp),
+                ("betas", vp), ("thresholds", vp)]
+
+
+class BatchRunArgs(C.Structure):
+    _fields_ = [("n_rounds", C.c_int32), ("sweeps_per_round", C.c_int32), ("round_offset", C.c_int64),
+                ("seed", C.c_uint64), ("items", vp), ("n_items", C.c_int32), ("max_tile", C.c_int32),
+                ("threads_per_slot", C.c_int32), ("ctas_per_sm", C.c_int32), ("positions_per_item", C.c_int32),
+                ("max_item_bytes", C.c_int32), ("timeout_s", C.c_double)]
+
+
 _lib = None
 
 
@@ -105,6 +121,11 @@ def load():
                                C.c_size_t, vp]
     L.drift_pt_run_noalloc.argtypes = [C.POINTER(DeviceProblem), C.POINTER(RunArgs), C.POINTER(DeviceState), vp]
     L.drift_pt_check.argtypes = [vp, vp]
+    L.drift_pt_batch_items.argtypes = [C.c_int32, vp, vp, C.c_int32, C.c_int64, vp, C.POINTER(C.c_int32)]
+    L.drift_pt_batch_init.argtypes = [C.POINTER(BatchProblem), C.POINTER(BatchRunArgs), C.POINTER(DeviceState), vp]
+    L.drift_pt_batch_workspace_bytes.argtypes = [C.POINTER(BatchProblem), C.POINTER(C.c_size_t)]
+    L.drift_pt_batch_run.argtypes = [C.POINTER(BatchProblem), C.POINTER(BatchRunArgs), C.POINTER(DeviceState), vp,
+                                     C.c_size_t, vp]
     L.drift_pt_energy_fp64.argtypes = [C.POINTER(DeviceProblem), vp, C.c_int32, vp, vp]
     L.drift_pt_solve.argtypes = [C.POINTER(Csr), C.POINTER(SolveArgs), C.POINTER(SolveResult)]
     for name in EXPORTED:

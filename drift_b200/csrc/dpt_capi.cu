@@ -4,12 +4,57 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <utility>
 #include <vector>
 
 #include "../../include/drift_pt.h"
 #include "dpt_common.cuh"
 #include "dpt_internal.h"
 #include "dpt_kernels.cuh"
+
+namespace dpt {
+
+int prepare_kernel(const void* fn, int threads, size_t smem, int* per_sm) {
+  struct Key {
+    const void* fn;
+    int dev, threads;
+    size_t smem;
+    bool operator<(const Key& o) const {
+      if (fn != o.fn) return fn < o.fn;
+      if (dev != o.dev) return dev < o.dev;
+      if (threads != o.threads) return threads < o.threads;
+      return smem < o.smem;
+    }
+  };
+  static std::mutex mu;
+  static std::map<Key, int> occ;
+  static std::map<std::pair<const void*, int>, size_t> smem_set;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  const Key key{fn, dev, threads, smem};
+  auto it = occ.find(key);
+  if (it != occ.end()) {
+    *per_sm = it->second;
+    return DRIFT_PT_OK;
+  }
+  size_t& cur = smem_set[std::make_pair(fn, dev)];
+  if (cur < smem) {
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return set_error(DRIFT_PT_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+    cur = smem;
+  }
+  int n = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, smem);
+  if (e != cudaSuccess) return set_error(DRIFT_PT_ECUDA, "occupancy query: %s", cudaGetErrorString(e));
+  occ[key] = n;
+  *per_sm = n;
+  return DRIFT_PT_OK;
+}
+
+}  // namespace dpt
 
 using namespace dpt;
 
@@ -192,11 +237,9 @@ int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPl
   lp->grid = (R + rpc - 1) / rpc;
   lp->smem = total(rpc, in_smem, threads);
   const void* fn = run_kernel_ptr(ip, lp->in_smem, p->max_width, p->min_width, p->has_field, lp->p);
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lp->smem);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
   int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, lp->smem);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+  rc = prepare_kernel(fn, threads, lp->smem, &per_sm);
+  if (rc) return rc;
   if ((long long)per_sm * di.sm_count < lp->grid)
     return set_error(DRIFT_PT_EUNSUPPORTED, "%d CTAs of %d threads / %zu B shared memory cannot be co-resident (%d per SM x %d SMs)",
                      lp->grid, threads, lp->smem, per_sm, di.sm_count);

@@ -15,4 +15,9 @@ constexpr int kMaxThreads = 512;
 int set_error(int code, const char* fmt, ...);
 void clear_error();
 
+// Raises the kernel's dynamic shared-memory limit to `smem` (if needed) and returns how many CTAs
+// of `threads` threads fit an SM. Results are cached per (kernel, threads, smem), so repeated
+// launches (and launches inside a stream capture) make no further attribute or occupancy calls.
+int prepare_kernel(const void* fn, int threads, size_t smem, int* per_sm);
+
 }  // namespace dpt

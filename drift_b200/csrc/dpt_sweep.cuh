@@ -1,0 +1,220 @@
+// dpt_sweep.cuh - the colour-phase item update shared by the single-ladder and batched kernels.
+//
+// One item is P consecutive positions (P = 8 or 4) of one replica: gather the local fields from
+// the sliced-ELL coupling table, draw the item's Philox block, apply the Metropolis test with the
+// 16+16-bit lazy uniforms, flip in shared memory and return the exact energy change.
+#pragma once
+#include <cstdint>
+
+#include "dpt_common.cuh"
+#include "dpt_internal.h"
+
+namespace dpt {
+
+// Shared memory is addressed through 32-bit byte offsets into the one dynamic shared array, so
+// every access compiles to a shared load/store with 32-bit address arithmetic.
+extern __shared__ __align__(16) unsigned char dpt_smem[];
+
+__device__ __forceinline__ uint32_t lds_u32(uint32_t off) { return *reinterpret_cast<const uint32_t*>(dpt_smem + off); }
+__device__ __forceinline__ int lds_s32(uint32_t off) { return *reinterpret_cast<const int*>(dpt_smem + off); }
+__device__ __forceinline__ float lds_f32(uint32_t off) { return *reinterpret_cast<const float*>(dpt_smem + off); }
+__device__ __forceinline__ int lds_s8(uint32_t off) { return (int)*reinterpret_cast<const int8_t*>(dpt_smem + off); }
+
+struct Tables {
+  // byte offsets in shared memory (tables staged in shared memory)
+  uint32_t soff_o, ent_o, nbr_o, wf_o, h_o;
+  // global pointers (tables read through L1/L2)
+  const int* soff;
+  const int* nbr;
+  const int8_t* w8;
+  const float* wf;
+  const void* h;
+};
+
+template <bool kInSmem>
+__device__ __forceinline__ int slice_off(const Tables& T, int S) {
+  if constexpr (kInSmem) return lds_s32(T.soff_o + 4u * (uint32_t)S);
+  else return __ldg(T.soff + S);
+}
+
+// P positions per item: sub-block b of group g covers positions 8g + P*b .. 8g + P*b + P-1. Every
+// item computes the group's whole Philox block and uses its own halves of it.
+template <int P> struct SpinWord;
+template <> struct SpinWord<8> { using T = uint64_t; };
+template <> struct SpinWord<4> { using T = uint32_t; };
+
+// Bits i of the result: position 8g + q0 + i lies in the colour range [lo, hi).
+template <int P>
+__device__ __forceinline__ uint32_t range_mask(int p0, int lo, int hi) {
+  const int a = min(max(lo - p0, 0), P), e = min(max(hi - p0, 0), P);
+  return ((1u << e) - 1u) & ~((1u << a) - 1u);
+}
+
+// Gather of the local fields of one item. W > 0 with kExactW: every slice has exactly W entries
+// per position, so all 2 * W * P shared loads are independent and issued before any use. W > 0
+// without kExactW: W bounds the width, loads beyond it are predicated off. W == 0: run-time loop.
+template <int W, bool kExactW, bool kInSmem, bool kField, int P>
+__device__ __forceinline__ void gather_int(int field[P], int S, int lane, int q0, uint32_t sp_o, const Tables& T) {
+  const int w0 = slice_off<kInSmem>(T, S);
+  const int width = kExactW ? W : slice_off<kInSmem>(T, S + 1) - w0;
+  const uint32_t base = (uint32_t)w0 * kSlicePositions + lane;
+#pragma unroll
+  for (int i = 0; i < P; ++i) {
+    const uint32_t hi_e = (uint32_t)(S * kSlicePositions + (q0 + i) * 32 + lane);
+    if constexpr (!kField) field[i] = 0;
+    else if constexpr (kInSmem) field[i] = lds_s32(T.h_o + 4u * hi_e);
+    else field[i] = __ldg(static_cast<const int*>(T.h) + hi_e);
+  }
+  if constexpr (W > 0) {
+    uint32_t ev[W][P];
+#pragma unroll
+    for (int d = 0; d < W; ++d)
+#pragma unroll
+      for (int i = 0; i < P; ++i) {
+        const uint32_t e = base + (uint32_t)d * kSlicePositions + (uint32_t)(q0 + i) * 32;
+        if (kExactW || d < width) {
+          if constexpr (kInSmem) ev[d][i] = lds_u32(T.ent_o + 4u * e);
+          else ev[d][i] = (uint32_t)__ldg(T.nbr + e) | ((uint32_t)(uint8_t)__ldg(T.w8 + e) << 24);
+        } else {
+          ev[d][i] = 0u;  // neighbour 0 with weight 0
+        }
+      }
+    int sv[W][P];
+#pragma unroll
+    for (int d = 0; d < W; ++d)
+#pragma unroll
+      for (int i = 0; i < P; ++i) sv[d][i] = lds_s8(sp_o + (ev[d][i] & 0xFFFFFFu));
+#pragma unroll
+    for (int d = 0; d < W; ++d)
+#pragma unroll
+      for (int i = 0; i < P; ++i) field[i] += (((int)ev[d][i]) >> 24) * sv[d][i];
+  } else {
+    for (int d = 0; d < width; ++d) {
+      uint32_t ev[P];
+#pragma unroll
+      for (int i = 0; i < P; ++i) {
+        const uint32_t e = base + (uint32_t)d * kSlicePositions + (uint32_t)(q0 + i) * 32;
+        if constexpr (kInSmem) ev[i] = lds_u32(T.ent_o + 4u * e);
+        else ev[i] = (uint32_t)__ldg(T.nbr + e) | ((uint32_t)(uint8_t)__ldg(T.w8 + e) << 24);
+      }
+#pragma unroll
+      for (int i = 0; i < P; ++i) field[i] += (((int)ev[i]) >> 24) * lds_s8(sp_o + (ev[i] & 0xFFFFFFu));
+    }
+  }
+}
+
+// sp_o: byte offset of the slot's spins; thr_o: byte offset of entry x = 0 of its rung's
+// extended threshold row (entries x = -F..F; x <= 0 is accepted before the lookup).
+template <int W, bool kExactW, bool kInSmem, bool kField, int P>
+__device__ __forceinline__ int group_int(int g, int b, int lo, int hi, uint32_t t, uint32_t slot, uint32_t sp_o,
+                                         const Tables& T, uint32_t thr_o, uint32_t c_sweep, uint32_t c_second,
+                                         uint32_t k0, uint32_t k1) {
+  using SW = typename SpinWord<P>::T;
+  const int q0 = P * b;
+  const int S = g >> 5, lane = g & 31;
+  int field[P];
+  gather_int<W, kExactW, kInSmem, kField, P>(field, S, lane, q0, sp_o, T);
+  const U4 rnd = philox(U4{(uint32_t)g, t, slot, c_sweep}, k0, k1);
+  const uint32_t words[4] = {rnd.x, rnd.y, rnd.z, rnd.w};
+  const uint32_t own_o = sp_o + (uint32_t)(g * kGroup + q0);
+  uint64_t s8 = (uint64_t)*reinterpret_cast<const SW*>(dpt_smem + own_o);
+  const uint32_t inmask = range_mask<P>(g * kGroup + q0, lo, hi);
+  int dacc = 0;
+#pragma unroll
+  for (int i = 0; i < P; ++i) {
+    const int q = q0 + i;
+    const int si = (int)(int8_t)(uint8_t)(s8 >> (8 * i));
+    const int x = si * field[i];
+    const uint32_t thr = lds_u32(thr_o + 4u * (uint32_t)x);
+    const uint32_t word = (P == 8) ? words[i >> 1] : (b ? words[2 + (i >> 1)] : words[i >> 1]);
+    const uint32_t prim = (word >> ((i & 1) * 16)) & 0xFFFFu;
+    const uint32_t th = thr >> 16;
+    const bool in = (inmask >> i) & 1u;
+    bool acc = (x <= 0) | (prim < th);
+    if (in & (x > 0) & (prim == th)) {  // the first 16 bits tie: draw the second half of this uniform
+      const U4 r2 = philox(U4{(uint32_t)(g * kGroup + q), t, slot, c_second}, k0, k1);
+      acc = (r2.x & 0xFFFFu) < (thr & 0xFFFFu);
+    }
+    acc = acc & in;
+    s8 ^= acc ? ((uint64_t)0xFEu << (8 * i)) : 0ull;  // +1 (0x01) <-> -1 (0xFF)
+    dacc += acc ? 2 * x : 0;
+  }
+  *reinterpret_cast<SW*>(dpt_smem + own_o) = (SW)s8;
+  return dacc;
+}
+
+template <int W, bool kExactW, bool kInSmem, bool kField>
+__device__ __forceinline__ void gather_f32(float field[kGroup], int S, int lane, uint32_t sp_o, const Tables& T) {
+  const int w0 = slice_off<kInSmem>(T, S);
+  const int width = kExactW ? W : slice_off<kInSmem>(T, S + 1) - w0;
+  const uint32_t base = (uint32_t)w0 * kSlicePositions + lane;
+#pragma unroll
+  for (int q = 0; q < kGroup; ++q) {
+    const uint32_t hi_e = (uint32_t)(S * kSlicePositions + q * 32 + lane);
+    if constexpr (!kField) field[q] = 0.0f;
+    else if constexpr (kInSmem) field[q] = lds_f32(T.h_o + 4u * hi_e);
+    else field[q] = __ldg(static_cast<const float*>(T.h) + hi_e);
+  }
+  // the sum runs over d in order (the fp32 rounding sequence is part of the definition)
+  auto step = [&](int d) {
+    int nb[kGroup];
+    float wt[kGroup];
+#pragma unroll
+    for (int q = 0; q < kGroup; ++q) {
+      const uint32_t e = base + (uint32_t)d * kSlicePositions + q * 32;
+      if constexpr (kInSmem) {
+        nb[q] = lds_s32(T.nbr_o + 4u * e);
+        wt[q] = lds_f32(T.wf_o + 4u * e);
+      } else {
+        nb[q] = __ldg(T.nbr + e);
+        wt[q] = __ldg(T.wf + e);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kGroup; ++q) field[q] = f_add(field[q], lds_s8(sp_o + (uint32_t)nb[q]) > 0 ? wt[q] : -wt[q]);
+  };
+  if constexpr (W > 0) {
+#pragma unroll
+    for (int d = 0; d < W; ++d)
+      if (kExactW || d < width) step(d);
+  } else {
+    for (int d = 0; d < width; ++d) step(d);
+  }
+}
+
+template <int W, bool kExactW, bool kInSmem, bool kField>
+__device__ __forceinline__ long long group_f32(int g, int lo, int hi, uint32_t t, uint32_t slot, uint32_t sp_o,
+                                               const Tables& T, float neg2beta, uint32_t c_sweep,
+                                               uint32_t c_second, uint32_t k0, uint32_t k1) {
+  const int S = g >> 5, lane = g & 31;
+  float field[kGroup];
+  gather_f32<W, kExactW, kInSmem, kField>(field, S, lane, sp_o, T);
+  const U4 rnd = philox(U4{(uint32_t)g, t, slot, c_sweep}, k0, k1);
+  const uint32_t words[4] = {rnd.x, rnd.y, rnd.z, rnd.w};
+  const uint32_t own_o = sp_o + (uint32_t)(g * kGroup);
+  uint64_t s8 = *reinterpret_cast<const uint64_t*>(dpt_smem + own_o);
+  const uint32_t inmask = range_mask<kGroup>(g * kGroup, lo, hi);
+  long long dacc = 0;
+#pragma unroll
+  for (int q = 0; q < kGroup; ++q) {
+    const int si = (int)(int8_t)(uint8_t)(s8 >> (8 * q));
+    const float x = si > 0 ? field[q] : -field[q];
+    const bool in = (inmask >> q) & 1u;
+    const bool pos = x > 0.0f;
+    const uint32_t thr = threshold_f(neg2beta, pos ? x : 0.0f);
+    const uint32_t prim = (words[q >> 1] >> ((q & 1) * 16)) & 0xFFFFu;
+    const uint32_t th = thr >> 16;
+    bool acc = (!pos) | (prim < th);
+    if (in & pos & (prim == th)) {
+      const U4 r2 = philox(U4{(uint32_t)(g * kGroup + q), t, slot, c_second}, k0, k1);
+      acc = (r2.x & 0xFFFFu) < (thr & 0xFFFFu);
+    }
+    acc = acc & in;
+    s8 ^= acc ? ((uint64_t)0xFEu << (8 * q)) : 0ull;
+    dacc += acc ? f_to_ll_rn(f_mul(x, 2.0f * kFloatEnergyQuant)) : 0ll;
+  }
+  *reinterpret_cast<uint64_t*>(dpt_smem + own_o) = s8;
+  return dacc;
+}
+
+}  // namespace dpt

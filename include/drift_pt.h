@@ -211,6 +211,82 @@ DRIFT_PT_API int drift_pt_energy_fp64(const DriftPtDeviceProblem* prob, const in
                          double* out, void* stream);
 
 /* ---------------------------------------------------------------------------------------------
+ * Batched layer: many independent instances (each its own couplings, colouring, size, ladder and
+ * replica count) advanced together by one persistent launch per call. No counterpart in the
+ * reference (its engine runs one instance per process, drift/gpu.py:97). Instance k is the same
+ * chain as a single-instance run with instance = desc[k].stream_id, so batching never changes
+ * results. All pointers are device memory. The per-instance layout arrays are the single-instance
+ * layout arrays concatenated; desc[k] holds the offsets.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct DriftPtInstanceDesc {
+  int32_t n, n_pos, n_slices, n_colors;
+  int32_t n_replicas;        /* R_k                                                         */
+  int32_t max_field;         /* F_k (integer path)                                          */
+  int32_t stream_id;         /* Philox stream of the instance (< 2^24)                      */
+  int32_t reserved;
+  int64_t color_ptr;         /* element offset of the instance's color_ptr[k+1]             */
+  int64_t slice_off;         /* element offset of its slice_off[n_slices+1]                 */
+  int64_t ell;               /* element offset of its ELL entries (slice_off is relative)   */
+  int64_t pos;               /* element offset of its h_pos[n_pos]                          */
+  int64_t slot0;             /* first replica slot of the instance in the batch             */
+  int64_t spin0;             /* byte offset of its spins [R_k][n_pos] in the spin arrays     */
+  int64_t thr;               /* element offset of its thresholds [R_k][F_k] (integer path)  */
+} DriftPtInstanceDesc;
+
+typedef struct DriftPtBatchProblem {
+  int32_t n_instances;
+  int32_t integer_path;      /* the same path for every instance of a batch                 */
+  int32_t has_field;         /* 1 if any instance has a non-zero field                      */
+  int32_t max_width;         /* largest slice width over the batch                          */
+  int32_t min_width;         /* smallest slice width over the batch                         */
+  int32_t max_field;         /* largest F_k                                                 */
+  int32_t max_n_pos;         /* largest n_pos                                               */
+  int32_t max_colors;        /* largest colour count                                        */
+  int64_t total_slots;       /* sum of R_k                                                  */
+  const DriftPtInstanceDesc* desc; /* [n_instances]                                         */
+  const int32_t* color_ptr;
+  const int32_t* slice_off;
+  const int32_t* ell_nbr;
+  const void* ell_w;
+  const void* h_pos;
+  const double* betas;       /* [total_slots]: beta of rung r of instance k at slot0_k + r  */
+  const uint32_t* thresholds;/* integer path: [R_k][F_k] per instance at desc.thr           */
+} DriftPtBatchProblem;
+
+/* Work items: one item = replicas [first, first + count) of one instance, processed by one CTA
+ * for a round. items[3*i] = instance, items[3*i+1] = first local slot, items[3*i+2] = count.
+ * Order them largest first for load balance (drift_pt_batch_items does). */
+DRIFT_PT_API int drift_pt_batch_items(int32_t n_instances, const int32_t* n_pos, const int32_t* n_replicas,
+                                      int32_t max_tile, int64_t smem_budget, int32_t* items, int32_t* n_items);
+
+typedef struct DriftPtBatchRunArgs {
+  int32_t n_rounds, sweeps_per_round;
+  int64_t round_offset;
+  uint64_t seed;
+  const int32_t* items;      /* device [n_items][3]                                         */
+  int32_t n_items;
+  int32_t max_tile;          /* largest item count                                          */
+  int32_t threads_per_slot;  /* threads bound to each slot of an item: 1..32 power of two or
+                                a multiple of 32; max_tile * threads_per_slot <= 512        */
+  int32_t ctas_per_sm;       /* 0 = as many as fit                                          */
+  int32_t positions_per_item;/* 8 or 4 (integer path), 0 = auto                             */
+  int32_t max_item_bytes;    /* largest count * n_pos over the items (spins staged per item) */
+  double timeout_s;
+} DriftPtBatchRunArgs;
+
+/* Initial spins/energies of every instance (as drift_pt_init with instance = stream_id). The
+ * state arrays are the single-instance arrays of all instances concatenated (spins at spin0,
+ * per-slot arrays at slot0; swap_tried/accepted have one entry per slot, R_k - 1 used). */
+DRIFT_PT_API int drift_pt_batch_init(const DriftPtBatchProblem* prob, const DriftPtBatchRunArgs* args,
+                                     DriftPtDeviceState* state, void* stream);
+DRIFT_PT_API int drift_pt_batch_workspace_bytes(const DriftPtBatchProblem* prob, size_t* bytes);
+/* n_rounds rounds of every instance: each round, CTAs take items from a queue and run the
+ * sweeps; a grid barrier; one warp per instance runs its exchange step; a grid barrier. */
+DRIFT_PT_API int drift_pt_batch_run(const DriftPtBatchProblem* prob, const DriftPtBatchRunArgs* args,
+                                    DriftPtDeviceState* state, void* workspace, size_t workspace_bytes,
+                                    void* stream);
+
+/* ---------------------------------------------------------------------------------------------
  * Host convenience: one call from host buffers to host results (the problem.bin -> result.bin
  * contract of cuda/ising_pt.cu:159-243 and drift/gpu.py:83-114). Allocates and frees device
  * memory internally; synchronous.

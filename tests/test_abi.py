@@ -154,3 +154,42 @@ def test_invalid_inputs_are_rejected_with_a_message():
     # device entry points reject NULL problems before touching the GPU
     assert L.drift_pt_init(None, None, None, None) == _lib.EINVAL
     assert L.drift_pt_run(None, None, None, None, 0, None) == _lib.EINVAL
+
+
+def test_ctypes_structs_match_the_header(tmp_path):
+    """Every struct of include/drift_pt.h has the same size and field offsets as its ctypes mirror."""
+    import shutil
+    import subprocess
+
+    from drift_b200.batch import DESC_DTYPE
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    mirrors = {"DriftPtCsr": _lib.Csr, "DriftPtLayoutInfo": _lib.LayoutInfo, "DriftPtLayout": _lib.Layout,
+               "DriftPtDeviceProblem": _lib.DeviceProblem, "DriftPtDeviceState": _lib.DeviceState,
+               "DriftPtRunArgs": _lib.RunArgs, "DriftPtSolveArgs": _lib.SolveArgs,
+               "DriftPtSolveResult": _lib.SolveResult, "DriftPtBatchProblem": _lib.BatchProblem,
+               "DriftPtBatchRunArgs": _lib.BatchRunArgs}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "drift_pt.h"', "int main(void) {"]
+    for cname, py in mirrors.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'printf("{cname}.{fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append('printf("DriftPtInstanceDesc size %zu\\n", sizeof(DriftPtInstanceDesc));')
+    for fname in DESC_DTYPE.names:
+        lines.append(f'printf("DriftPtInstanceDesc.{fname} %zu\\n", offsetof(DriftPtInstanceDesc, {fname}));')
+    lines.append("return 0; }")
+    src = tmp_path / "probe.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "probe"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)], check=True)
+    got = dict(l.rsplit(" ", 1) for l in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                         check=True).stdout.splitlines())
+    for cname, py in mirrors.items():
+        assert int(got[f"{cname} size"]) == C.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert int(got[f"{cname}.{fname}"]) == getattr(py, fname).offset, f"{cname}.{fname}"
+    assert int(got["DriftPtInstanceDesc size"]) == DESC_DTYPE.itemsize
+    for fname in DESC_DTYPE.names:
+        assert int(got[f"DriftPtInstanceDesc.{fname}"]) == DESC_DTYPE.fields[fname][1], fname
