@@ -39,7 +39,22 @@ WORKLOADS = {
                        n=4096, seed=2, R=64, beta=(0.2, 4.0), sweeps=100000, spr=4, bytes_per_attempt=2.0 + 3 * 5 / 64),
     "ea2d": dict(desc="2D EA +-J L=16 periodic (N=256), 24 replicas, beta 0.1-3.0, 2e4 sweeps, swap every sweep",
                  n=256, seed=1, R=24, beta=(0.1, 3.0), sweeps=20000, spr=1, bytes_per_attempt=2.0 + 4 * 5 / 24),
+    # batched: 512 Erdos-Renyi instances, N ~ U{64..8192}, mean degree 6, J ~ N(0,1) fp32, h ~ N(0, 0.1),
+    # 32 replicas each on a geometric beta ladder 0.1-3.0; 5e4 sweeps per job (one step times 100 rounds
+    # of 5 sweeps, 1 % of the job: the full job takes about a minute per run)
+    "batched_er": dict(desc="512 ER instances N~U[64,8192], deg 6, Gaussian J fp32, h~N(0,0.1), 32 replicas each, "
+                            "beta 0.1-3.0; 500 of the job's 5e4 sweeps per step",
+                       n_instances=512, seed=3, R=32, beta=(0.1, 3.0), sweeps=500, spr=5,
+                       bytes_per_attempt=2.0 + 6 * 8 / 32 + 4 / 32),
 }
+
+
+def make_batch_models(w):
+    from drift_b200.instances import er_gaussian
+
+    rng = np.random.default_rng(w["seed"])
+    sizes = rng.integers(64, 8193, size=w["n_instances"])
+    return [er_gaussian(int(n), 6, 1000 + i, field_sigma=0.1) for i, n in enumerate(sizes)]
 
 
 def make_model(name):
@@ -341,6 +356,100 @@ def bench_b200(args):
         dist.destroy_process_group()
 
 
+def bench_batched(args):
+    import torch
+
+    from drift_b200.batch import BatchEngine, BatchProblem, autotune
+    from drift_b200.engine import HostProblem
+
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    w = WORKLOADS[args.workload]
+    t_build0 = time.perf_counter()
+    models = make_batch_models(w)
+    hps = [HostProblem.from_model(m, order="degree") for m in models]
+    ladders = [ladder(w)] * len(hps)
+    bp = BatchProblem(hps, ladders, stream_ids=np.arange(len(hps)) + 1024 * rank, device=dev)
+    t_build = time.perf_counter() - t_build0
+    rounds = args.rounds or w["sweeps"] // w["spr"]
+    eng = BatchEngine(bp, seed=1, sweeps_per_round=w["spr"])
+    eng.init()
+    shape = autotune(eng, rounds=2)
+    total_n = int(sum(int(d["n"]) for d in bp.desc))
+    attempts_per_step = float(w["R"]) * total_n * rounds * w["spr"]
+    # the timed step is a replay of a captured CUDA graph of the step's rounds (10 launches)
+    eng.run(1)
+    torch.cuda.synchronize()
+    chunk = max(1, rounds // 10)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        done = 0
+        while done < rounds:
+            c = min(chunk, rounds - done)
+            eng.run(c)
+            done += c
+    for _ in range(args.warmup):
+        g.replay()
+    eng.check()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    t_steps = 0.0
+    for s_ in range(args.steps):
+        flush.fill_(s_ & 0xFF)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        g.replay()
+        e1.record()
+        e1.synchronize()
+        t_steps += e0.elapsed_time(e1) * 1e-3
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    eng.check()
+    t_max = reduce_max(t_steps, world, dev)
+    value = attempts_per_step * args.steps * world / t_max / 1e9
+    # end to end through the public Python API: layouts and state uploaded from host, run, best
+    # energies downloaded
+    t0 = time.perf_counter()
+    bp2 = BatchProblem(hps, ladders, stream_ids=np.arange(len(hps)) + 1024 * rank, device=dev)
+    e2 = BatchEngine(bp2, seed=2, sweeps_per_round=w["spr"], **shape)
+    e2.init()
+    e2.run(rounds)
+    best = e2.best_energies()
+    t_e2e = reduce_max(time.perf_counter() - t0, world, dev)
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        achieved = attempts_per_step * w["bytes_per_attempt"] / (t_max / args.steps) / 1e9
+        h2d = int(sum(t.numel() * t.element_size() for t in (bp2.d_desc, bp2.d_color_ptr, bp2.d_slice_off,
+                                                             bp2.d_ell_nbr, bp2.d_ell_w, bp2.d_h_pos, bp2.d_betas)))
+        line = {
+            "metric": "spin-flips/ns", "value": value, "unit": "flips/ns", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": w["desc"], "instances": len(hps), "total_spins": total_n, "rounds": rounds,
+                       "sweeps_per_round": w["spr"], "attempts_per_step": attempts_per_step,
+                       "parallelism": f"replicas-only x{world}", "l2": "flushed between steps (256 MiB write)",
+                       "launch": shape, "cuda_graph": True, "host_build_s": t_build},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": load_traffic("pt_batched_kernel/batched_er"), "peak_kind": peak_kind,
+                         "kernel": "pt_batched_kernel", "bytes_per_attempt": w["bytes_per_attempt"]},
+            "e2e": {"value": attempts_per_step * world / t_e2e / 1e9, "unit": "flips/ns", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": int(bp2.total_slots * 8), "api": "BatchProblem + BatchEngine (Python)",
+                    "best_energy_mean": float(np.mean(best))},
+            "gpu_launches": 10 * args.steps,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -354,6 +463,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         bench_reference(args)
+    elif args.workload == "batched_er":
+        bench_batched(args)
     else:
         bench_b200(args)
 

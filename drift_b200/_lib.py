@@ -20,7 +20,7 @@ EXPORTED = (
     "drift_pt_layout_query", "drift_pt_layout_fill", "drift_pt_thresholds", "drift_pt_workspace_bytes",
     "drift_pt_init", "drift_pt_run", "drift_pt_check", "drift_pt_energy_fp64", "drift_pt_solve",
     "drift_pt_run_noalloc", "drift_pt_batch_items", "drift_pt_batch_init", "drift_pt_batch_workspace_bytes",
-    "drift_pt_batch_run",
+    "drift_pt_batch_run", "drift_pt_ms_workspace_bytes", "drift_pt_ms_init", "drift_pt_ms_run",
 )
 
 vp = C.c_void_p

@@ -78,7 +78,12 @@ DPT_HD U4 philox(U4 c, uint32_t k0, uint32_t k1) {
 //   kTagSwap  : ctr = (r, round lo, round hi, .) -> words 0,1 form a 53-bit uniform for the
 //               exchange of rungs r, r+1 in that round.
 // ---------------------------------------------------------------------------------------------
-constexpr uint32_t kTagSweep = 1u, kTagSecond = 2u, kTagInit = 3u, kTagSwap = 4u;
+//   kTagMsSweep: multispin lattices (32 replicas per word), ctr = (q, t, (w << 8) | (p >> 2), .),
+//               word (p & 3) is random bit-plane p (p = 0 most significant) of the 32 uniforms
+//               u_b = sum_p bit_b(plane_p) 2^(31-p) of site q (colour-split index), word w.
+//   kTagMsInit : ctr = (q, 0, w, .) word 0 = the initial bits of site q in word w (1 = spin -1).
+constexpr uint32_t kTagSweep = 1u, kTagSecond = 2u, kTagInit = 3u, kTagSwap = 4u, kTagMsSweep = 5u,
+                   kTagMsInit = 6u;
 constexpr uint32_t kMaxInstance = (1u << 24) - 1u;
 
 DPT_HD uint32_t ctr3(uint32_t tag, uint32_t instance) { return (tag << 24) | (instance & kMaxInstance); }

@@ -51,9 +51,21 @@ class HostProblem:
     color_spins: np.ndarray
 
     @classmethod
-    def from_model(cls, model) -> "HostProblem":
+    def from_model(cls, model, order: str = "index") -> "HostProblem":
+        """Greedy colouring of the model's couplings (drift/gpu.py:122-145). ``order`` sets the
+        order of the spins inside each colour class: "index" (the reference's stable order) or
+        "degree" (descending degree, then index), which gives slices of nearly uniform width on
+        irregular graphs. Any order inside a class is an equally valid sweep; the uniforms follow
+        the positions, so runs are reproducible for a given order."""
         n, row_ptr, col_idx, weight, h = model_csr(model)
         _, color_ptr, color_spins = greedy_coloring(n, row_ptr, col_idx)
+        if order == "degree":
+            deg = np.diff(row_ptr)
+            for c in range(len(color_ptr) - 1):
+                seg = color_spins[color_ptr[c]:color_ptr[c + 1]]
+                color_spins[color_ptr[c]:color_ptr[c + 1]] = seg[np.lexsort((seg, -deg[seg]))]
+        elif order != "index":
+            raise ValueError("order must be 'index' or 'degree'")
         return cls(n, row_ptr, col_idx, weight, h, color_ptr, color_spins)
 
     @property

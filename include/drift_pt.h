@@ -287,6 +287,55 @@ DRIFT_PT_API int drift_pt_batch_run(const DriftPtBatchProblem* prob, const Drift
                                     void* stream);
 
 /* ---------------------------------------------------------------------------------------------
+ * Multispin layer: +-J cubic lattices (d = 2 or 3, even side L, periodic, no field) with 32
+ * replicas packed per 32-bit word. No counterpart in the reference: its engine stores one float
+ * per spin per replica and a CSR of J (cuda/ising_pt.cu:47-52,190-191), and a 3-D L = 64 lattice
+ * cannot even be built as its dense IsingModel (drift/ising.py:32).
+ *   Sites are split by checkerboard colour c = (x + y + z) & 1: q = c * N/2 + (x >> 1)
+ *   + (L/2) * (y + L * z). Spin words [W][N]: bit b of word w at q is replica slot 32 w + b,
+ *   1 = spin -1. jneg[q] bit d (d = 0: +x, 1: +y, 2: +z) is set when J(site, site + e_d) = -1.
+ *   Thresholds: [R][2d] from drift_pt_thresholds(R, betas, 2d, ...) (a flip with k unsatisfied
+ *   bonds has dE = 4 (d - k); k >= d is always accepted).
+ * ------------------------------------------------------------------------------------------- */
+typedef struct DriftPtLattice {
+  int32_t dims, L;
+  const uint8_t* jneg;       /* device [N]                                                  */
+} DriftPtLattice;
+
+typedef struct DriftPtMsState { /* device arrays; R = 32 * n_words */
+  uint32_t* words;           /* [W][N]                                                      */
+  uint32_t* best_words;      /* [W][N]: bit b holds replica b's lowest-energy configuration  */
+  int64_t* energy;           /* [R] exact, E = -sum_bonds J s s                             */
+  int64_t* best_energy;      /* [R]                                                         */
+  int32_t* rung_of_slot;     /* [R]                                                         */
+  int32_t* slot_of_rung;     /* [R]                                                         */
+  int64_t* swap_tried;       /* [R-1]                                                       */
+  int64_t* swap_accepted;    /* [R-1]                                                       */
+} DriftPtMsState;
+
+typedef struct DriftPtMsRunArgs {
+  int32_t n_words;           /* W (replicas R = 32 W), 1..64                                */
+  int32_t n_rounds, sweeps_per_round;
+  int32_t ctas_per_sm;       /* 0 = 2                                                       */
+  int64_t round_offset;
+  uint64_t seed;
+  uint32_t instance;
+  int32_t reserved;
+  const double* betas;       /* [R] device                                                  */
+  const uint32_t* thresholds;/* [R][2d] device                                              */
+  double timeout_s;
+} DriftPtMsRunArgs;
+
+DRIFT_PT_API int drift_pt_ms_workspace_bytes(int32_t n_words, size_t* bytes);
+/* Random initial words (Philox), exact energies, best = initial, identity rungs. */
+DRIFT_PT_API int drift_pt_ms_init(const DriftPtLattice* lat, const DriftPtMsRunArgs* args, DriftPtMsState* state,
+                                  void* stream);
+/* n_rounds rounds of (sweeps_per_round checkerboard sweeps of all replicas, exact energy
+ * recount, per-replica best update, adjacent-rung exchange). One persistent launch. */
+DRIFT_PT_API int drift_pt_ms_run(const DriftPtLattice* lat, const DriftPtMsRunArgs* args, DriftPtMsState* state,
+                                 void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------------------------------------------
  * Host convenience: one call from host buffers to host results (the problem.bin -> result.bin
  * contract of cuda/ising_pt.cu:159-243 and drift/gpu.py:83-114). Allocates and frees device
  * memory internally; synchronous.

@@ -40,7 +40,7 @@ _lib = None
 
 
 def build(force: bool = False) -> str:
-    srcs = [os.path.join(HERE, f) for f in ("pt_oracle.c", "exact.c", "Makefile")]
+    srcs = [os.path.join(HERE, f) for f in ("pt_oracle.c", "exact.c", "ms_oracle.c", "Makefile")]
     if force or not os.path.exists(LIB_PATH) or any(os.path.getmtime(s) > os.path.getmtime(LIB_PATH) for s in srcs):
         r = subprocess.run(["make", "-s", "-C", HERE, "-B" if force else "all"], capture_output=True, text=True)
         if r.returncode != 0:
@@ -72,6 +72,15 @@ class _ExactOut(C.Structure):
                 ("spectrum", C.c_void_p)]
 
 
+class _MsOracle(C.Structure):
+    _fields_ = [("dims", C.c_int32), ("L", C.c_int32), ("W", C.c_int32), ("jneg", C.c_void_p), ("betas", C.c_void_p),
+                ("thr", C.c_void_p), ("seed", C.c_uint64), ("instance", C.c_uint32), ("n_rounds", C.c_int32),
+                ("spr", C.c_int32), ("init", C.c_int32), ("round_offset", C.c_int64), ("words", C.c_void_p),
+                ("best_words", C.c_void_p), ("energy", C.c_void_p), ("best_energy", C.c_void_p),
+                ("rung_of_slot", C.c_void_p), ("slot_of_rung", C.c_void_p), ("tried", C.c_void_p),
+                ("accepted", C.c_void_p)]
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -92,6 +101,8 @@ def lib():
         L.oracle_threshold_int.restype = C.c_uint32
         L.oracle_energy_fp64.argtypes = [C.POINTER(_Problem), C.c_void_p]
         L.oracle_energy_fp64.restype = C.c_double
+        L.oracle_ms_run.argtypes = [C.POINTER(_MsOracle)]
+        L.oracle_ms_run.restype = C.c_int
         _lib = L
     return _lib
 
@@ -236,3 +247,38 @@ def exact(J: np.ndarray, h: np.ndarray, betas=(), spectrum: bool = False, site_m
         raise ValueError("oracle_exact: n must be in 1..30")
     return ExactResult(out.e_min, out.argmin, me[:nb], me2[:nb], ma[:nb], mm2[:nb],
                        sm[:nb] if sm is not None else None, spec)
+
+
+class MsState:
+    def __init__(self, W: int, N: int):
+        R = 32 * W
+        self.words = np.zeros((W, N), np.uint32)
+        self.best_words = np.zeros((W, N), np.uint32)
+        self.energy = np.zeros(R, np.int64)
+        self.best_energy = np.zeros(R, np.int64)
+        self.rung_of_slot = np.arange(R, dtype=np.int32)
+        self.slot_of_rung = np.arange(R, dtype=np.int32)
+        self.tried = np.zeros(max(R - 1, 1), np.int64)
+        self.accepted = np.zeros(max(R - 1, 1), np.int64)
+
+
+def ms_run(dims: int, L: int, jneg: np.ndarray, betas, *, n_rounds: int, sweeps_per_round: int, seed: int,
+           instance: int = 0, state: MsState | None = None, round_offset: int = 0) -> MsState:
+    """The multispin lattice chain (ms_oracle.c): jneg in colour-split site order, R = len(betas)."""
+    betas = np.ascontiguousarray(betas, np.float64)
+    R = len(betas)
+    if R % 32:
+        raise ValueError("multispin needs a multiple of 32 replicas")
+    W, N = R // 32, L ** dims
+    jneg = np.ascontiguousarray(jneg, np.uint8)
+    thr = np.ascontiguousarray(thresholds(betas, 2 * dims), np.uint32)
+    init = state is None
+    if state is None:
+        state = MsState(W, N)
+    o = _MsOracle(dims, L, W, _p(jneg), _p(betas), _p(thr), seed & 0xFFFFFFFFFFFFFFFF, instance, n_rounds,
+                  sweeps_per_round, 1 if init else 0, round_offset, _p(state.words), _p(state.best_words),
+                  _p(state.energy), _p(state.best_energy), _p(state.rung_of_slot), _p(state.slot_of_rung),
+                  _p(state.tried), _p(state.accepted))
+    if lib().oracle_ms_run(C.byref(o)) != 0:
+        raise ValueError("oracle_ms_run failed")
+    return state

@@ -68,6 +68,28 @@ def test_batch_matches_single_instance_runs(which):
             assert np.array_equal(got[key], ref[key]), f"instance {k}: {key}"
 
 
+def test_degree_ordered_layout_matches_oracle():
+    model = er_gaussian(3000, 6, 11)
+    hp = HostProblem.from_model(model, order="degree")
+    deg = np.diff(hp.row_ptr)
+    for c in range(hp.n_colors):
+        seg = hp.color_spins[hp.color_ptr[c]:hp.color_ptr[c + 1]]
+        assert np.all(np.diff(deg[seg]) <= 0)
+    betas = geometric_betas(8, 1 / 3.0, 10.0)
+    bp = BatchProblem([hp], [betas], stream_ids=[3])
+    eng = BatchEngine(bp, seed=5, sweeps_per_round=2)
+    eng.init()
+    eng.run(7)
+    eng.check()
+    prob = oracle.OracleProblem(hp.n, hp.row_ptr, hp.col_idx, hp.weight, hp.h, hp.color_ptr, hp.color_spins,
+                                integer_path=False)
+    ost = oracle.pt_run(prob, betas, n_rounds=7, sweeps_per_round=2, seed=5, instance=3)
+    got = eng.fetch(0)
+    assert np.array_equal(got["spins"], ost.spins)
+    assert np.array_equal(got["energy_fixed"], ost.energy)
+    assert np.array_equal(got["accepted"], ost.accepted[:7])
+
+
 def test_batch_instance_matches_oracle():
     models, ladders = int_batch()
     rounds, spr, seed = 10, 2, 4
