@@ -23,8 +23,27 @@
 
 namespace dpt {
 
+// n / d for 32-bit n: the high 64 bits of n * m with m = floor((2^64 - 1) / d) + 1 (exact for
+// every 32-bit n and d >= 2, since n * d < 2^64); d == 1 is the identity.
+struct FastDiv {
+  unsigned long long m;
+  unsigned int d;
+};
+
+__host__ __device__ inline FastDiv make_fastdiv(unsigned int d) {
+  FastDiv f;
+  f.d = d;
+  f.m = d > 1 ? (~0ull / d) + 1ull : 0ull;
+  return f;
+}
+
+__device__ __forceinline__ unsigned int fdiv(unsigned int n, const FastDiv& f) {
+  return f.d == 1 ? n : (unsigned int)__umul64hi((unsigned long long)n, f.m);
+}
+
 struct MsArgs {
   int dims, L, W, R, half, n_sites;  // half = L/2, n_sites = L^dims
+  FastDiv div_half, div_L;
   const uint8_t* jneg;
   int n_rounds, spr;
   long long round0;
@@ -115,11 +134,11 @@ struct Coord {
 
 __device__ __forceinline__ Coord ms_coord(const MsArgs& a, int c, int h) {
   Coord p;
-  const int xh = h % a.half;
-  const int rest = h / a.half;
+  const int rest = (int)fdiv((unsigned)h, a.div_half);
+  const int xh = h - rest * a.half;
   if (a.dims == 3) {
-    p.y = rest % a.L;
-    p.z = rest / a.L;
+    p.z = (int)fdiv((unsigned)rest, a.div_L);
+    p.y = rest - p.z * a.L;
   } else {
     p.y = rest;
     p.z = 0;
@@ -272,72 +291,121 @@ __global__ void __launch_bounds__(256) ms_run_kernel(const MsArgs a) {
   rebuild_planes();
   __syncthreads();
   const int n2 = a.n_sites / 2;
-  const long long gtid = (long long)blockIdx.x * B + tid, gsz = (long long)gridDim.x * B;
+  const int gtid = blockIdx.x * B + tid, gsz = gridDim.x * B;
+  const int lane = tid & 31;
   const uint32_t cms = ctr3(kTagMsSweep, a.inst);
   unsigned long long nsync = 0;
+  for (int i = tid; i < R; i += B) cnt_sm[i] = 0;
+  __syncthreads();
   for (int j = 0; j < a.n_rounds; ++j) {
     const long long round = a.round0 + j;
     for (int sw = 0; sw < a.spr; ++sw) {
       const uint32_t t = (uint32_t)(round * a.spr + sw);
       for (int c = 0; c < 2; ++c) {
-        for (long long task = gtid; task < (long long)W * n2; task += gsz) {
-          const int w = (int)(task / n2), h = (int)(task - (long long)w * n2);
-          const Coord p = ms_coord(a, c, h);
-          const int q = c * n2 + h;
+        // the round's last phase also counts, per replica, the unsatisfied bonds of every colour-1
+        // site after its update: each bond has exactly one colour-1 end, so the sum is the total
+        const bool count = (sw == a.spr - 1) && (c == 1);
+        for (int w = 0; w < W; ++w) {
           uint32_t* wb = a.words + (size_t)w * a.n_sites;
-          const uint32_t s = __ldcg(wb + q);
-          const int xp = p.x + 1 == a.L ? 0 : p.x + 1, xm = p.x == 0 ? a.L - 1 : p.x - 1;
-          const int yp = p.y + 1 == a.L ? 0 : p.y + 1, ym = p.y == 0 ? a.L - 1 : p.y - 1;
-          const uint8_t jb = __ldg(a.jneg + q);
-          const int q_xm = ms_q(a, xm, p.y, p.z), q_ym = ms_q(a, p.x, ym, p.z);
-          uint32_t u[6];
-          u[0] = s ^ __ldcg(wb + ms_q(a, xp, p.y, p.z)) ^ ((jb & 1) ? ~0u : 0u);
-          u[1] = s ^ __ldcg(wb + q_xm) ^ ((__ldg(a.jneg + q_xm) & 1) ? ~0u : 0u);
-          u[2] = s ^ __ldcg(wb + ms_q(a, p.x, yp, p.z)) ^ ((jb & 2) ? ~0u : 0u);
-          u[3] = s ^ __ldcg(wb + q_ym) ^ ((__ldg(a.jneg + q_ym) & 2) ? ~0u : 0u);
-          if (dims == 3) {
-            const int zp = p.z + 1 == a.L ? 0 : p.z + 1, zm = p.z == 0 ? a.L - 1 : p.z - 1;
-            const int q_zm = ms_q(a, p.x, p.y, zm);
-            u[4] = s ^ __ldcg(wb + ms_q(a, p.x, p.y, zp)) ^ ((jb & 4) ? ~0u : 0u);
-            u[5] = s ^ __ldcg(wb + q_zm) ^ ((__ldg(a.jneg + q_zm) & 4) ? ~0u : 0u);
-          }
-          uint32_t k0, k1, k2;
-          ms_count(u, 2 * dims, k0, k1, k2);
-          // class masks: m[k] for the k < dims classes that need a test
-          uint32_t m[3];
-          m[0] = ~(k0 | k1 | k2);
-          m[1] = k0 & ~k1 & ~k2;
-          m[2] = ~k0 & k1 & ~k2;
-          const uint32_t need = dims == 3 ? (m[0] | m[1] | m[2]) : (m[0] | m[1]);
-          uint32_t lt = 0, und = need;
           const uint32_t* pl = planes + (w * dims) * 32;
-          for (int ch = 0; ch < 8 && und; ++ch) {
-            const U4 r = philox(U4{(uint32_t)q, t, ((uint32_t)w << 8) | (uint32_t)ch, cms}, a.k0, a.k1);
-            const uint32_t rw[4] = {r.x, r.y, r.z, r.w};
+          uint32_t cs[16];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-              const int pp = ch * 4 + i;
-              uint32_t tp = (m[0] & pl[pp]) | (m[1] & pl[32 + pp]);
-              if (dims == 3) tp |= m[2] & pl[64 + pp];
-              lt |= und & ~rw[i] & tp;
-              und &= ~(rw[i] ^ tp);
+          for (int p = 0; p < 16; ++p) cs[p] = 0u;
+          for (int h = gtid; h < n2; h += gsz) {
+            const Coord p = ms_coord(a, c, h);
+            const int q = c * n2 + h;
+            const uint32_t s = __ldcg(wb + q);
+            const int xp = p.x + 1 == a.L ? 0 : p.x + 1, xm = p.x == 0 ? a.L - 1 : p.x - 1;
+            const int yp = p.y + 1 == a.L ? 0 : p.y + 1, ym = p.y == 0 ? a.L - 1 : p.y - 1;
+            const uint8_t jb = __ldg(a.jneg + q);
+            const int q_xm = ms_q(a, xm, p.y, p.z), q_ym = ms_q(a, p.x, ym, p.z);
+            uint32_t u[6];
+            u[0] = s ^ __ldcg(wb + ms_q(a, xp, p.y, p.z)) ^ ((jb & 1) ? ~0u : 0u);
+            u[1] = s ^ __ldcg(wb + q_xm) ^ ((__ldg(a.jneg + q_xm) & 1) ? ~0u : 0u);
+            u[2] = s ^ __ldcg(wb + ms_q(a, p.x, yp, p.z)) ^ ((jb & 2) ? ~0u : 0u);
+            u[3] = s ^ __ldcg(wb + q_ym) ^ ((__ldg(a.jneg + q_ym) & 2) ? ~0u : 0u);
+            if (dims == 3) {
+              const int zp = p.z + 1 == a.L ? 0 : p.z + 1, zm = p.z == 0 ? a.L - 1 : p.z - 1;
+              const int q_zm = ms_q(a, p.x, p.y, zm);
+              u[4] = s ^ __ldcg(wb + ms_q(a, p.x, p.y, zp)) ^ ((jb & 4) ? ~0u : 0u);
+              u[5] = s ^ __ldcg(wb + q_zm) ^ ((__ldg(a.jneg + q_zm) & 4) ? ~0u : 0u);
+            }
+            uint32_t k0, k1, k2;
+            ms_count(u, 2 * dims, k0, k1, k2);
+            // class masks: m[k] for the k < dims classes that need a test
+            uint32_t m[3];
+            m[0] = ~(k0 | k1 | k2);
+            m[1] = k0 & ~k1 & ~k2;
+            m[2] = ~k0 & k1 & ~k2;
+            const uint32_t need = dims == 3 ? (m[0] | m[1] | m[2]) : (m[0] | m[1]);
+            uint32_t lt = 0, und = need;
+            for (int ch = 0; ch < 8 && und; ++ch) {
+              const U4 r = philox(U4{(uint32_t)q, t, ((uint32_t)w << 8) | (uint32_t)ch, cms}, a.k0, a.k1);
+              const uint32_t rw[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+              for (int i = 0; i < 4; ++i) {
+                const int pp = ch * 4 + i;
+                uint32_t tp = (m[0] & pl[pp]) | (m[1] & pl[32 + pp]);
+                if (dims == 3) tp |= m[2] & pl[64 + pp];
+                lt |= und & ~rw[i] & tp;
+                und &= ~(rw[i] ^ tp);
+              }
+            }
+            const uint32_t acc = (~need) | lt;
+            wb[q] = s ^ acc;
+            if (count) {
+              // unsatisfied bonds after the update: 2d - k where the bit flipped, k otherwise
+              uint32_t d0, d1, d2;
+              if (dims == 3) {  // 6 - k
+                d0 = k0;
+                d1 = ~(k1 ^ k0);
+                d2 = ~(k2 ^ (k1 & k0));
+              } else {  // 4 - k
+                d0 = k0;
+                d1 = k1 ^ k0;
+                d2 = ~(k2 ^ (k1 | k0));
+              }
+              const uint32_t add[3] = {(acc & d0) | (~acc & k0), (acc & d1) | (~acc & k1), (acc & d2) | (~acc & k2)};
+#pragma unroll
+              for (int b = 0; b < 3; ++b) {
+                uint32_t v = add[b];
+#pragma unroll
+                for (int pp = b; pp < 16; ++pp) {
+                  const uint32_t tcar = cs[pp] & v;
+                  cs[pp] ^= v;
+                  v = tcar;
+                }
+              }
             }
           }
-          const uint32_t acc = (~need) | lt;
-          wb[q] = s ^ acc;
+          if (count) {
+            // per-replica totals: bit b of plane p summed over the warp's lanes, weight 2^p
+            unsigned int mine = 0;
+#pragma unroll
+            for (int pp = 0; pp < 16; ++pp) {
+              if (!__any_sync(0xffffffffu, cs[pp] != 0u)) continue;
+#pragma unroll 8
+              for (int b = 0; b < 32; ++b) {
+                const unsigned int v = __ballot_sync(0xffffffffu, (cs[pp] >> b) & 1u);
+                if (lane == b) mine += (unsigned int)__popc(v) << pp;
+              }
+            }
+            if (mine) atomicAdd(cnt_sm + w * 32 + lane, mine);
+          }
+        }
+        if (count) {
+          __syncthreads();
+          unsigned long long* ec = a.ecnt + (size_t)(round & 1) * R;
+          for (int i = tid; i < R; i += B) {
+            if (cnt_sm[i]) atomicAdd(ec + i, (unsigned long long)cnt_sm[i]);
+            cnt_sm[i] = 0;
+          }
         }
         if (!ms_grid_sync(a, ++nsync, ctl)) return;
       }
     }
-    // ---- round end: exact energies from the unsatisfied bonds of every replica ----
-    for (int i = tid; i < R; i += B) cnt_sm[i] = 0;
-    __syncthreads();
-    ms_count_unsat(a, cnt_sm);
-    __syncthreads();
+    // ---- round end: exact energies from the unsatisfied-bond counts ----
     unsigned long long* ec = a.ecnt + (size_t)(round & 1) * R;
-    for (int i = tid; i < R; i += B)
-      if (cnt_sm[i]) atomicAdd(ec + i, (unsigned long long)cnt_sm[i]);
-    if (!ms_grid_sync(a, ++nsync, ctl)) return;
     const long long bonds = (long long)dims * a.n_sites;
     for (int i = tid; i < R; i += B) eall[i] = 2 * (long long)__ldcg(ec + i) - bonds;
     for (int i = tid; i < W; i += B) imp[i] = 0;
@@ -351,10 +419,12 @@ __global__ void __launch_bounds__(256) ms_run_kernel(const MsArgs a) {
       for (int i = tid; i < R; i += B) a.ecnt[(size_t)((round + 1) & 1) * R + i] = 0;
     __syncthreads();
     // best configurations: copy the improved replicas' bits
-    for (long long task = gtid; task < (long long)W * a.n_sites; task += gsz) {
-      const int w = (int)(task / a.n_sites);
+    for (int w = 0; w < W; ++w) {
       const uint32_t mk = imp[w];
-      if (mk) a.best_words[task] = (__ldcg(a.best_words + task) & ~mk) | (__ldcg(a.words + task) & mk);
+      if (!mk) continue;
+      uint32_t* bw = a.best_words + (size_t)w * a.n_sites;
+      const uint32_t* cw = a.words + (size_t)w * a.n_sites;
+      for (int q = gtid; q < a.n_sites; q += gsz) bw[q] = (__ldcg(bw + q) & ~mk) | (__ldcg(cw + q) & mk);
     }
     // exchange step (identical in every CTA)
     if (tid < 32) {
@@ -437,6 +507,8 @@ MsArgs ms_args(const DriftPtLattice* lat, const DriftPtMsRunArgs* r, DriftPtMsSt
   a.R = 32 * r->n_words;
   a.half = lat->L / 2;
   a.n_sites = lat->L * lat->L * (lat->dims == 3 ? lat->L : 1);
+  a.div_half = make_fastdiv((unsigned)a.half);
+  a.div_L = make_fastdiv((unsigned)lat->L);
   a.jneg = lat->jneg;
   a.n_rounds = r->n_rounds;
   a.spr = r->sweeps_per_round;
@@ -514,6 +586,12 @@ extern "C" int drift_pt_ms_run(const DriftPtLattice* lat, const DriftPtMsRunArgs
   if (per_sm < 1) return set_error(DRIFT_PT_EUNSUPPORTED, "multispin kernel does not fit an SM");
   const int want = args->ctas_per_sm > 0 ? args->ctas_per_sm : 2;  // fewer CTAs: cheaper grid barriers
   per_sm = per_sm < want ? per_sm : want;
+  {
+    // each thread's bit-sliced bond counter has 16 planes: its sites per word times 2d must stay below 2^16
+    const long long threads_total = (long long)per_sm * sms * threads;
+    const long long per_thread = (a.n_sites / 2 + threads_total - 1) / threads_total;
+    if (per_thread * 2 * a.dims >= 65536) return set_error(DRIFT_PT_EUNSUPPORTED, "multispin: lattice too large for the grid");
+  }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   cudaError_t e = cudaMemsetAsync(ws, 0, need, st);
   if (e != cudaSuccess) return ms_fail(e, "workspace reset");
