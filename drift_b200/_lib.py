@@ -21,6 +21,8 @@ EXPORTED = (
     "drift_pt_init", "drift_pt_run", "drift_pt_check", "drift_pt_energy_fp64", "drift_pt_solve",
     "drift_pt_run_noalloc", "drift_pt_batch_items", "drift_pt_batch_init", "drift_pt_batch_workspace_bytes",
     "drift_pt_batch_run", "drift_pt_ms_workspace_bytes", "drift_pt_ms_init", "drift_pt_ms_run",
+    "drift_pt_sk_quantize", "drift_pt_sk_layout_bytes", "drift_pt_sk_layout_fill", "drift_pt_sk_scales",
+    "drift_pt_sk_workspace_bytes", "drift_pt_sk_init", "drift_pt_sk_run", "drift_pt_sk_energy",
 )
 
 vp = C.c_void_p

@@ -18,7 +18,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB_PATH = os.path.join(HERE, "libdrift_pt.so")
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-SOURCES = ["dpt_host.cpp", "dpt_kernels.cu", "dpt_capi.cu", "dpt_noalloc.cu", "dpt_batched.cu", "dpt_multispin.cu"]
+SOURCES = ["dpt_host.cpp", "dpt_kernels.cu", "dpt_capi.cu", "dpt_noalloc.cu", "dpt_batched.cu", "dpt_multispin.cu",
+           "dpt_sk_host.cpp", "dpt_sk.cu"]
 
 
 def nvcc() -> str:

@@ -82,8 +82,11 @@ DPT_HD U4 philox(U4 c, uint32_t k0, uint32_t k1) {
 //               word (p & 3) is random bit-plane p (p = 0 most significant) of the 32 uniforms
 //               u_b = sum_p bit_b(plane_p) 2^(31-p) of site q (colour-split index), word w.
 //   kTagMsInit : ctr = (q, 0, w, .) word 0 = the initial bits of site q in word w (1 = spin -1).
+//   kTagSkSweep: dense couplings, ctr = (((i >> 7) << 5) | (i & 31), t, slot, .), word ((i >> 5) & 3)
+//               is the uniform of spin i in sweep t (one Philox call covers spins i, i+32, i+64,
+//               i+96 of a 128-spin tile).
 constexpr uint32_t kTagSweep = 1u, kTagSecond = 2u, kTagInit = 3u, kTagSwap = 4u, kTagMsSweep = 5u,
-                   kTagMsInit = 6u;
+                   kTagMsInit = 6u, kTagSkSweep = 7u;
 constexpr uint32_t kMaxInstance = (1u << 24) - 1u;
 
 DPT_HD uint32_t ctr3(uint32_t tag, uint32_t instance) { return (tag << 24) | (instance & kMaxInstance); }
@@ -158,6 +161,14 @@ DPT_HD float f_fma(float a, float b, float c) {
   return __fmaf_rn(a, b, c);
 #else
   return fmaf(a, b, c);
+#endif
+}
+DPT_HD float f_div(float a, float b) {
+#if defined(__CUDA_ARCH__)
+  return __fdiv_rn(a, b);
+#else
+  volatile float r = a / b;
+  return r;
 #endif
 }
 DPT_HD float f_rint(float a) { return rintf(a); }
@@ -266,6 +277,52 @@ DPT_HD uint32_t threshold_int(double beta, int x) {
   double v = d_mul(e, 4294967296.0);
   if (v >= 4294967295.0) return 0xFFFFFFFFu;
   return (uint32_t)v;  // truncation = floor for v >= 0
+}
+
+// ---------------------------------------------------------------------------------------------
+// -ln(u) for u in [2^-24, 1), float. u = m 2^e with m in (sqrt(2)/2, sqrt(2)]; with
+// z = (m - 1) / (m + 1), ln m = 2 atanh z = 2 z (1 + z^2/3 + z^4/5 + z^6/7 + z^8/9)
+// (|z| <= 0.1716, truncation < 2^-28 relative); ln u = e ln2 + ln m.
+// ---------------------------------------------------------------------------------------------
+DPT_HD float neg_log_unit_f(float u) {
+  uint32_t bits;
+#if defined(__CUDA_ARCH__)
+  bits = __float_as_uint(u);
+#else
+  memcpy(&bits, &u, sizeof bits);
+#endif
+  int e = (int)(bits >> 23) - 127;
+  uint32_t mb = (bits & 0x007FFFFFu) | 0x3F800000u;
+  if (mb > 0x3FB504F3u) {  // m > sqrt(2): halve it
+    mb -= 0x00800000u;
+    e += 1;
+  }
+  const float m = bits_to_float(mb);
+  const float z = f_div(f_sub(m, 1.0f), f_add(m, 1.0f));
+  const float w = f_mul(z, z);
+  float p = f_fma(w, 0x1.c71c72p-4f, 0x1.24924ap-3f);  // 1/9, 1/7
+  p = f_fma(w, p, 0x1.99999ap-3f);                     // 1/5
+  p = f_fma(w, p, 0x1.555556p-2f);                     // 1/3
+  p = f_fma(w, p, 1.0f);
+  const float lnm = f_mul(f_add(z, z), p);
+  const float r = -f_fma((float)e, 0x1.62e430p-1f, lnm);  // ln 2 rounded to float
+  return r > 0.0f ? r : 0.0f;
+}
+
+// Dense-coupling acceptance. Spin i with integer local field F (couplings and field in units of
+// 2^-shift) is flipped iff s_i F <= D, D = floor(-ln(u) * c), c = 2^shift / (2 beta) rounded to
+// float, u = (2 (word >> 9) + 1) 2^-24. That is dE = 2 s_i F 2^-shift <= -ln(u) / beta, i.e.
+// u <= exp(-beta dE): the Metropolis rule, with the transcendental taken off the spin-to-spin
+// dependency chain (D depends only on the uniform and the rung).
+DPT_HD int32_t sk_threshold(uint32_t word, float c) {
+  const float u = f_mul((float)(2u * (word >> 9) + 1u), 0x1.0p-24f);
+  const float v = f_mul(neg_log_unit_f(u), c);
+  if (v >= 2147483648.0f) return 2147483647;
+#if defined(__CUDA_ARCH__)
+  return __float2int_rz(v);
+#else
+  return (int32_t)v;
+#endif
 }
 
 // Fixed-point scale of the energy accumulators: the integer path stores E exactly (scale 1); the

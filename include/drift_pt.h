@@ -336,6 +336,80 @@ DRIFT_PT_API int drift_pt_ms_run(const DriftPtLattice* lat, const DriftPtMsRunAr
                                  void* workspace, size_t workspace_bytes, void* stream);
 
 /* ---------------------------------------------------------------------------------------------
+ * Dense layer: fully connected couplings (Sherrington-Kirkpatrick type), n <= 512, R <= 512.
+ * The reference runs such models through the same CSR kernel as sparse ones
+ * (cuda/ising_pt.cu:109-122): every spin is its own colour class and each attempt walks n - 1
+ * neighbours. Here the chain keeps every replica's local fields F = J s + h exact in integer
+ * fixed point and updates them on the tensor cores.
+ *   Couplings: Jq = rint(J 2^shift), hq = rint(h 2^shift) (int32), shift chosen by
+ *   drift_pt_sk_quantize so that |Jq| < 2^23 - 2^16 and every |F| < 2^30.
+ *   Sweep: spins 0..n-1 in order; spin i flips iff s_i F_i <= D, D = floor(-ln(u) scale[rung])
+ *   with scale[rung] = float(2^shift / (2 beta_rung)) (drift_pt_sk_scales) and u from word
+ *   ((i >> 5) & 3) of Philox(((i >> 7) << 5 | (i & 31), t, slot, 7 << 24 | instance)).
+ *   Energies are exact int64 in units of 2^-(shift+1): E2 = -sum_i s_i (sum_j Jq_ij s_j + 2 hq_i).
+ *   Rounds, best tracking and the adjacent-rung exchange are those of drift_pt_run (the exchange
+ *   uses E = E2 2^-(shift+1)).
+ * Device coupling table: drift_pt_sk_layout_fill writes, for every block of 32 spins, the 24-bit
+ * couplings of those 32 columns as three int8 limbs (Jq = d0 + 2^8 d1 + 2^16 d2, each in
+ * [-128, 127]) in the tensor cores' shared-memory operand layout, followed by two 32 x 32 int32
+ * blocks: the diagonal block and the couplings to the previous block of the sweep.
+ * ------------------------------------------------------------------------------------------- */
+#define DRIFT_PT_SK_MAX_N 512
+#define DRIFT_PT_SK_MAX_R 512
+
+typedef struct DriftPtSkProblem {
+  int32_t n;
+  int32_t shift;
+  const int32_t* Jq;         /* device [n][n] symmetric, zero diagonal                       */
+  const int32_t* hq;         /* device [n]                                                   */
+  const void* layout;        /* device, drift_pt_sk_layout_bytes(n) bytes                    */
+} DriftPtSkProblem;
+
+typedef struct DriftPtSkState { /* device arrays */
+  int8_t* spins;             /* [R][n] +-1, natural spin order                               */
+  int8_t* best_spins;        /* [R][n]                                                       */
+  int64_t* energy;           /* [R] E2 (units 2^-(shift+1))                                  */
+  int64_t* best_energy;      /* [R]                                                          */
+  int32_t* rung_of_slot;     /* [R]                                                          */
+  int32_t* slot_of_rung;     /* [R]                                                          */
+  int64_t* swap_tried;       /* [R-1]                                                        */
+  int64_t* swap_accepted;    /* [R-1]                                                        */
+  int64_t* best_history;     /* [n_rounds] or NULL: lowest E2 seen up to each round          */
+} DriftPtSkState;
+
+typedef struct DriftPtSkRunArgs {
+  int32_t n_replicas;
+  int32_t n_rounds, sweeps_per_round;
+  int32_t replicas_per_cta;  /* 1..12; 0 = automatic                                        */
+  int64_t round_offset;
+  uint64_t seed;
+  uint32_t instance;
+  int32_t reserved;
+  const double* betas;       /* [R] device                                                   */
+  const float* scales;       /* [R] device, drift_pt_sk_scales                               */
+  double timeout_s;
+} DriftPtSkRunArgs;
+
+/* Host: choose shift and quantise (J [n][n] symmetric with zero diagonal, h [n] or NULL). */
+DRIFT_PT_API int drift_pt_sk_quantize(int32_t n, const double* J, const double* h, int32_t* Jq, int32_t* hq,
+                                      int32_t* shift);
+DRIFT_PT_API int drift_pt_sk_layout_bytes(int32_t n, size_t* bytes);
+DRIFT_PT_API int drift_pt_sk_layout_fill(int32_t n, const int32_t* Jq, void* layout);
+/* Host: scale[r] = float(2^shift / (2 betas[r])). */
+DRIFT_PT_API int drift_pt_sk_scales(int32_t n_replicas, const double* betas, int32_t shift, float* scales);
+DRIFT_PT_API int drift_pt_sk_workspace_bytes(int32_t n_replicas, size_t* bytes);
+/* Random initial spins (the Philox init of drift_pt_init, in natural order), exact energies,
+ * best = initial, identity rungs, zero exchange counts. */
+DRIFT_PT_API int drift_pt_sk_init(const DriftPtSkProblem* problem, const DriftPtSkRunArgs* args,
+                                  DriftPtSkState* state, void* stream);
+/* n_rounds rounds in one persistent launch. */
+DRIFT_PT_API int drift_pt_sk_run(const DriftPtSkProblem* problem, const DriftPtSkRunArgs* args,
+                                 DriftPtSkState* state, void* workspace, size_t workspace_bytes, void* stream);
+/* Exact E2 of R configurations [R][n] (check). */
+DRIFT_PT_API int drift_pt_sk_energy(const DriftPtSkProblem* problem, int32_t n_replicas, const int8_t* spins,
+                                    int64_t* energy, void* stream);
+
+/* ---------------------------------------------------------------------------------------------
  * Host convenience: one call from host buffers to host results (the problem.bin -> result.bin
  * contract of cuda/ising_pt.cu:159-243 and drift/gpu.py:83-114). Allocates and frees device
  * memory internally; synchronous.

@@ -13,7 +13,9 @@ product (``drift_b200``) imports this package.
                             driven by the same counter-based uniforms as the engine, so spins,
                             energies and swap counts can be compared bit for bit;
       - ``exact``           drift/solvers/exact.py:20-49 as a Gray-code walk (n <= 30), plus
-                            Boltzmann averages.
+                            Boltzmann averages;
+      - ``ms_run``          the bit-packed lattice chain (ms_oracle.c);
+      - ``sk_run``          the dense-coupling chain on fixed-point couplings (sk_oracle.c).
   * ``ref_pt`` - NumPy restatement of the reference CPU parallel tempering
     (drift/solvers/parallel_tempering.py:29-124) with the same NumPy random stream, pinned to the
     reference by golden outputs in tests/golden/.
@@ -40,7 +42,7 @@ _lib = None
 
 
 def build(force: bool = False) -> str:
-    srcs = [os.path.join(HERE, f) for f in ("pt_oracle.c", "exact.c", "ms_oracle.c", "Makefile")]
+    srcs = [os.path.join(HERE, f) for f in ("pt_oracle.c", "exact.c", "ms_oracle.c", "sk_oracle.c", "Makefile")]
     if force or not os.path.exists(LIB_PATH) or any(os.path.getmtime(s) > os.path.getmtime(LIB_PATH) for s in srcs):
         r = subprocess.run(["make", "-s", "-C", HERE, "-B" if force else "all"], capture_output=True, text=True)
         if r.returncode != 0:
@@ -81,6 +83,16 @@ class _MsOracle(C.Structure):
                 ("accepted", C.c_void_p)]
 
 
+class _SkOracle(C.Structure):
+    _fields_ = [("n", C.c_int32), ("R", C.c_int32), ("n_rounds", C.c_int32), ("spr", C.c_int32), ("init", C.c_int32),
+                ("threads", C.c_int32), ("Jq", C.c_void_p), ("hq", C.c_void_p), ("betas", C.c_void_p),
+                ("scales", C.c_void_p), ("escale", C.c_double), ("seed", C.c_uint64), ("instance", C.c_uint32),
+                ("reserved", C.c_int32), ("round_offset", C.c_int64), ("spins", C.c_void_p),
+                ("best_spins", C.c_void_p), ("energy", C.c_void_p), ("best_energy", C.c_void_p),
+                ("rung_of_slot", C.c_void_p), ("slot_of_rung", C.c_void_p), ("tried", C.c_void_p),
+                ("accepted", C.c_void_p), ("best_history", C.c_void_p)]
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -103,6 +115,14 @@ def lib():
         L.oracle_energy_fp64.restype = C.c_double
         L.oracle_ms_run.argtypes = [C.POINTER(_MsOracle)]
         L.oracle_ms_run.restype = C.c_int
+        L.oracle_sk_run.argtypes = [C.POINTER(_SkOracle)]
+        L.oracle_sk_run.restype = C.c_int
+        L.oracle_sk_energy.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oracle_sk_energy.restype = C.c_int64
+        L.oracle_neg_log_unit.argtypes = [C.c_float]
+        L.oracle_neg_log_unit.restype = C.c_float
+        L.oracle_sk_threshold.argtypes = [C.c_uint32, C.c_float]
+        L.oracle_sk_threshold.restype = C.c_int32
         _lib = L
     return _lib
 
@@ -281,4 +301,56 @@ def ms_run(dims: int, L: int, jneg: np.ndarray, betas, *, n_rounds: int, sweeps_
                   _p(state.tried), _p(state.accepted))
     if lib().oracle_ms_run(C.byref(o)) != 0:
         raise ValueError("oracle_ms_run failed")
+    return state
+
+
+def neg_log_unit(u: float) -> float:
+    return float(lib().oracle_neg_log_unit(u))
+
+
+def sk_threshold(word: int, c: float) -> int:
+    return int(lib().oracle_sk_threshold(word & 0xFFFFFFFF, c))
+
+
+def sk_energy(Jq: np.ndarray, hq: np.ndarray, spins: np.ndarray) -> int:
+    """E2 = -sum_i s_i (sum_j Jq_ij s_j + 2 hq_i), exact."""
+    Jq = np.ascontiguousarray(Jq, np.int32)
+    hq = np.ascontiguousarray(hq, np.int32)
+    s = np.ascontiguousarray(spins, np.int8)
+    return int(lib().oracle_sk_energy(len(hq), _p(Jq), _p(hq), _p(s)))
+
+
+class SkState:
+    def __init__(self, R: int, n: int):
+        self.spins = np.zeros((R, n), np.int8)
+        self.best_spins = np.zeros((R, n), np.int8)
+        self.energy = np.zeros(R, np.int64)
+        self.best_energy = np.zeros(R, np.int64)
+        self.rung_of_slot = np.arange(R, dtype=np.int32)
+        self.slot_of_rung = np.arange(R, dtype=np.int32)
+        self.tried = np.zeros(R, np.int64)
+        self.accepted = np.zeros(R, np.int64)
+        self.best_history = None
+
+
+def sk_run(Jq: np.ndarray, hq: np.ndarray, shift: int, betas, scales, *, n_rounds: int, sweeps_per_round: int,
+           seed: int, instance: int = 0, state: SkState | None = None, round_offset: int = 0,
+           threads: int = 0) -> SkState:
+    """The dense-coupling chain (sk_oracle.c) on fixed-point couplings Jq, hq; R = len(betas)."""
+    Jq = np.ascontiguousarray(Jq, np.int32)
+    hq = np.ascontiguousarray(hq, np.int32)
+    betas = np.ascontiguousarray(betas, np.float64)
+    scales = np.ascontiguousarray(scales, np.float32)
+    n, R = len(hq), len(betas)
+    init = state is None
+    if state is None:
+        state = SkState(R, n)
+    hist = np.zeros(max(n_rounds, 1), np.int64)
+    o = _SkOracle(n, R, n_rounds, sweeps_per_round, 1 if init else 0, threads, _p(Jq), _p(hq), _p(betas), _p(scales),
+                  2.0 ** -(shift + 1), seed & 0xFFFFFFFFFFFFFFFF, instance, 0, round_offset, _p(state.spins),
+                  _p(state.best_spins), _p(state.energy), _p(state.best_energy), _p(state.rung_of_slot),
+                  _p(state.slot_of_rung), _p(state.tried), _p(state.accepted), _p(hist))
+    if lib().oracle_sk_run(C.byref(o)) != 0:
+        raise ValueError("oracle_sk_run failed")
+    state.best_history = hist[:n_rounds]
     return state

@@ -162,6 +162,8 @@ def test_ctypes_structs_match_the_header(tmp_path):
     import subprocess
 
     from drift_b200.batch import DESC_DTYPE
+    from drift_b200.multispin import LatticeC, MsRunArgsC, MsStateC
+    from drift_b200.sk import SkProblemC, SkRunArgsC, SkStateC
 
     cc = shutil.which("gcc") or shutil.which("cc")
     if cc is None:
@@ -170,7 +172,9 @@ def test_ctypes_structs_match_the_header(tmp_path):
                "DriftPtDeviceProblem": _lib.DeviceProblem, "DriftPtDeviceState": _lib.DeviceState,
                "DriftPtRunArgs": _lib.RunArgs, "DriftPtSolveArgs": _lib.SolveArgs,
                "DriftPtSolveResult": _lib.SolveResult, "DriftPtBatchProblem": _lib.BatchProblem,
-               "DriftPtBatchRunArgs": _lib.BatchRunArgs}
+               "DriftPtBatchRunArgs": _lib.BatchRunArgs, "DriftPtLattice": LatticeC, "DriftPtMsState": MsStateC,
+               "DriftPtMsRunArgs": MsRunArgsC, "DriftPtSkProblem": SkProblemC, "DriftPtSkState": SkStateC,
+               "DriftPtSkRunArgs": SkRunArgsC}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "drift_pt.h"', "int main(void) {"]
     for cname, py in mirrors.items():
         lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
