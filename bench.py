@@ -1,6 +1,7 @@
 """Benchmark: spin-flip attempts per ns of the B200 parallel-tempering engine.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload maxcut3reg|ea2d] [--impl b200|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload maxcut3reg|ea2d|batched_er|sk512]
+                    [--impl b200|reference]
 
 Workload (default ``maxcut3reg``): plain PT on MaxCut as Ising over a random 3-regular graph,
 N = 4096 (seeded), J = -1 on edges, h = 0, int8 spins, greedy colouring (4 colours), 64 replicas
@@ -46,6 +47,11 @@ WORKLOADS = {
                             "beta 0.1-3.0; 500 of the job's 5e4 sweeps per step",
                        n_instances=512, seed=3, R=32, beta=(0.1, 3.0), sweeps=500, spr=5,
                        bytes_per_attempt=2.0 + 6 * 8 / 32 + 4 / 32),
+    # dense SK: J_ij ~ N(0, 1)/sqrt(N) (fp32 values) on the upper triangle, mirrored, h = 0, seed 4;
+    # 64 replicas, beta 0.3-3.0, rounds of 10 sweeps; 1e4 sweeps per step. Tensor-core field
+    # updates: the algorithmic work of an attempt is the 2N flops of J_i . s (drift/ising.py:68)
+    "sk512": dict(desc="SK N=512, J~N(0,1/N) fp32, 64 replicas, beta 0.3-3.0, 1e4 sweeps in rounds of 10",
+                  n=512, seed=4, R=64, beta=(0.3, 3.0), sweeps=10000, spr=10, flops_per_attempt=2 * 512),
 }
 
 
@@ -58,9 +64,11 @@ def make_batch_models(w):
 
 
 def make_model(name):
-    from drift_b200.instances import ea_2d, maxcut_3regular
+    from drift_b200.instances import ea_2d, maxcut_3regular, sk_model
 
     w = WORKLOADS[name]
+    if name == "sk512":
+        return sk_model(w["n"], w["seed"])
     return maxcut_3regular(w["n"], w["seed"]) if name == "maxcut3reg" else ea_2d(16, w["seed"])
 
 
@@ -183,7 +191,8 @@ def run_reference_sample(args_tuple):
     from oracle import ref_pt
 
     w = WORKLOADS[name]
-    model = make_model(name).to_dense()
+    model = make_model(name)
+    model = model.to_dense() if hasattr(model, "to_dense") else model
     b = ladder(w)
     t0 = time.perf_counter()
     out = ref_pt.parallel_tempering(model, n_replicas=w["R"], T_min=1.0 / b[0], T_max=1.0 / b[-1], n_rounds=1,
@@ -356,6 +365,135 @@ def bench_b200(args):
         dist.destroy_process_group()
 
 
+def load_tensor_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("bf16_tflops_sustained", d.get("bf16_tflops"))), "measured (bf16 sustained)"
+    return 1400.0, "fallback (bf16 sustained)"
+
+
+def cpu_baseline_sk(w, sk, budget_s=12.0):
+    """The C oracle of the dense chain (OpenMP over replicas) on the host cores, bounded."""
+    import oracle
+
+    b = ladder(w)
+    sc = sk.scales(b)
+    threads = os.cpu_count() or 1
+    st = oracle.sk_run(sk.Jq, sk.hq, sk.shift, b, sc, n_rounds=1, sweeps_per_round=1, seed=3, threads=threads)
+    t0 = time.perf_counter()
+    rounds = 0
+    while time.perf_counter() - t0 < budget_s:
+        st = oracle.sk_run(sk.Jq, sk.hq, sk.shift, b, sc, n_rounds=1, sweeps_per_round=w["spr"], seed=3,
+                           threads=threads, state=st, round_offset=1 + rounds)
+        rounds += 1
+    dt = time.perf_counter() - t0
+    attempts = rounds * w["spr"] * w["R"] * w["n"]
+    return {"value": attempts / dt / 1e9, "unit": "flips/ns", "cores": threads, "kind": "port",
+            "sample": f"oracle/sk_oracle.c, {rounds} rounds x {w['spr']} sweeps x {w['R']} replicas x {w['n']} spins "
+                      f"({attempts:.3g} attempts, {dt:.1f} s), OpenMP over replicas"}
+
+
+def bench_sk(args):
+    import torch
+
+    from drift_b200.sk import SkEngine, SkModel
+
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    w = WORKLOADS[args.workload]
+    model = make_model(args.workload)
+    sk = SkModel.from_model(model)
+    betas = ladder(w)
+    rounds = args.rounds or w["sweeps"] // w["spr"]
+    eng = SkEngine(sk, betas, seed=1, sweeps_per_round=w["spr"], instance=rank, replicas_per_cta=args.sk_g,
+                   device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    attempts_per_step = float(w["R"]) * rounds * w["spr"] * w["n"]
+    ev_k0, ev_k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def step(seed):
+        eng.seed = seed
+        eng.init()
+        ev_k0.record()
+        eng.run(rounds)
+        ev_k1.record()
+
+    for s_ in range(args.warmup):
+        step(100 + s_)
+    eng.check()
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    t_steps, t_kernel = 0.0, 0.0
+    for s_ in range(args.steps):
+        flush.fill_(s_ & 0xFF)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step(1000 + s_)
+        e1.record()
+        e1.synchronize()
+        t_steps += e0.elapsed_time(e1) * 1e-3
+        t_kernel += ev_k0.elapsed_time(ev_k1) * 1e-3
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    eng.check()
+    best = eng.fetch()["best_energy"].min() * sk.energy_unit
+    t_max = reduce_max(t_steps, world, dev)
+    tk_max = reduce_max(t_kernel, world, dev)
+    value = attempts_per_step * args.steps * world / t_max / 1e9
+    # end to end through the public Python API: quantisation and coupling table on the host, upload,
+    # initialisation, the rounds, results downloaded
+    e2e_steps = max(1, min(args.steps, 3))
+    barrier(world)
+    t0 = time.perf_counter()
+    h2d = d2h = 0
+    for k in range(e2e_steps):
+        sk2 = SkModel.from_model(model)
+        e2 = SkEngine(sk2, betas, seed=7 + k, sweeps_per_round=w["spr"], instance=rank, replicas_per_cta=args.sk_g,
+                      device=dev)
+        e2.init()
+        e2.run(rounds)
+        out = e2.fetch()
+        h2d = sk2.Jq.nbytes + sk2.hq.nbytes + sk2.layout.nbytes + betas.nbytes + 4 * len(betas)
+        d2h = sum(v.nbytes for v in out.values() if isinstance(v, np.ndarray))
+    t_e2e = reduce_max(time.perf_counter() - t0, world, dev)
+    if rank == 0:
+        peak, peak_kind = load_tensor_peak()
+        launch_s = tk_max / args.steps
+        achieved = attempts_per_step * w["flops_per_attempt"] / launch_s / 1e12
+        line = {
+            "metric": "spin-flips/ns", "value": value, "unit": "flips/ns", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32 (int8 tensor-core limbs)", "data": "synthetic",
+            "config": {"workload": w["desc"] + (f" [shortened to {rounds} rounds]" if args.rounds else ""),
+                       "rounds": rounds, "sweeps_per_round": w["spr"], "attempts_per_step": attempts_per_step,
+                       "parallelism": f"replicas-only x{world}", "l2": "flushed between steps (256 MiB write)",
+                       "replicas_per_cta": eng.replicas_per_cta or "auto", "shift": sk.shift,
+                       "best_energy_last_step": float(best)},
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind, "kernel": "sk_run_kernel",
+                         "flops_per_attempt": w["flops_per_attempt"], "kernel_ms": launch_s * 1e3,
+                         "note": "sequential Metropolis chain: latency of the per-spin decision bounds the kernel"},
+            "e2e": {"value": attempts_per_step * e2e_steps * world / t_e2e / 1e9, "unit": "flips/ns",
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "api": "SkModel + SkEngine (Python over the C ABI), host J in, results out"},
+            "gpu_launches": 2 * args.steps,
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_sk(w, sk)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
 def bench_batched(args):
     import torch
 
@@ -458,6 +596,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="maxcut3reg", choices=list(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sk-g", type=int, default=4, help="dense workload: replicas per CTA (1..12)")
     ap.add_argument("--rounds", type=int, default=0,
                     help="override the rounds per step (profiling of a short case; the line then says so)")
     args = ap.parse_args()
@@ -465,6 +604,8 @@ def main():
         bench_reference(args)
     elif args.workload == "batched_er":
         bench_batched(args)
+    elif args.workload == "sk512":
+        bench_sk(args)
     else:
         bench_b200(args)
 
