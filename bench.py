@@ -1,6 +1,6 @@
 """Benchmark: spin-flip attempts per ns of the B200 parallel-tempering engine.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload maxcut3reg|ea2d|batched_er|sk512]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload maxcut3reg|ea2d|batched_er|ea3d64|sk512]
                     [--impl b200|reference]
 
 Workload (default ``maxcut3reg``): plain PT on MaxCut as Ising over a random 3-regular graph,
@@ -50,6 +50,13 @@ WORKLOADS = {
     # dense SK: J_ij ~ N(0, 1)/sqrt(N) (fp32 values) on the upper triangle, mirrored, h = 0, seed 4;
     # 64 replicas, beta 0.3-3.0, rounds of 10 sweeps; 1e4 sweeps per step. Tensor-core field
     # updates: the algorithmic work of an attempt is the 2N flops of J_i . s (drift/ising.py:68)
+    # 3-D Edwards-Anderson +-J, L = 64 periodic (N = 262,144), seed 5; 128 replicas packed 32 per
+    # word; beta 0.2-2.0; 1e4 sweeps in rounds of 10. Algorithmic bytes per attempt: spin read and
+    # write (2 bits) + 3 coupling bits per site shared by the 128 replicas = 0.253 B
+    "ea3d64": dict(desc="3D EA +-J L=64 periodic (N=262144), 128 replicas (bit-packed), beta 0.2-2.0, 1e4 sweeps "
+                        "in rounds of 10",
+                   n=64 ** 3, L=64, seed=5, R=128, beta=(0.2, 2.0), sweeps=10000, spr=10,
+                   bytes_per_attempt=2 / 8 + 3 / 8 / 128),
     "sk512": dict(desc="SK N=512, J~N(0,1/N) fp32, 64 replicas, beta 0.3-3.0, 1e4 sweeps in rounds of 10",
                   n=512, seed=4, R=64, beta=(0.3, 3.0), sweeps=10000, spr=10, flops_per_attempt=2 * 512),
 }
@@ -203,6 +210,11 @@ def run_reference_sample(args_tuple):
 def bench_reference(args):
     rank, world, local = dist_setup(args.gpus)
     if rank != 0:
+        return
+    if args.workload == "ea3d64":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference CPU PT needs the dense J of the "
+                          "L=64 lattice (262144^2 float64 = 550 GB); see the multispin oracle cpu_baseline instead"}),
+              flush=True)
         return
     import multiprocessing as mp
 
@@ -476,7 +488,8 @@ def bench_sk(args):
                        "replicas_per_cta": eng.replicas_per_cta or "auto", "shift": sk.shift,
                        "best_energy_last_step": float(best)},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind, "kernel": "sk_run_kernel",
+                         "frac": achieved / peak, "traffic": load_traffic("sk_run_kernel/sk512"), "peak_kind": peak_kind,
+                         "kernel": "sk_run_kernel",
                          "flops_per_attempt": w["flops_per_attempt"], "kernel_ms": launch_s * 1e3,
                          "note": "sequential Metropolis chain: latency of the per-spin decision bounds the kernel"},
             "e2e": {"value": attempts_per_step * e2e_steps * world / t_e2e / 1e9, "unit": "flips/ns",
@@ -487,6 +500,117 @@ def bench_sk(args):
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_sk(w, sk)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def cpu_baseline_ms(w, lat, budget_s=12.0):
+    """The multispin oracle (one replica bit at a time) on a bounded number of sweeps."""
+    import oracle
+
+    b = ladder(w)
+    t0 = time.perf_counter()
+    st = oracle.ms_run(3, w["L"], lat.jneg, b, n_rounds=1, sweeps_per_round=1, seed=3)
+    sweeps = 1
+    while time.perf_counter() - t0 < budget_s:
+        st = oracle.ms_run(3, w["L"], lat.jneg, b, n_rounds=1, sweeps_per_round=1, seed=3, state=st,
+                           round_offset=sweeps)
+        sweeps += 1
+    dt = time.perf_counter() - t0
+    attempts = sweeps * w["R"] * w["n"]
+    return {"value": attempts / dt / 1e9, "unit": "flips/ns", "cores": 1, "kind": "port",
+            "sample": f"oracle/ms_oracle.c (scalar, one replica bit at a time), {sweeps} sweeps x {w['R']} replicas x "
+                      f"{w['n']} sites incl. initialisation ({attempts:.3g} attempts, {dt:.1f} s)"}
+
+
+def bench_ms(args):
+    import torch
+
+    from drift_b200.multispin import Lattice, MsEngine
+
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    w = WORKLOADS[args.workload]
+    lat = Lattice.edwards_anderson(3, w["L"], w["seed"])
+    betas = ladder(w)
+    rounds = args.rounds or w["sweeps"] // w["spr"]
+    eng = MsEngine(lat, betas, seed=1, sweeps_per_round=w["spr"], instance=rank, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    attempts_per_step = float(w["R"]) * rounds * w["spr"] * w["n"]
+    ev_k0, ev_k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def step(seed):
+        eng.seed = seed
+        eng.init()
+        ev_k0.record()
+        eng.run(rounds)
+        ev_k1.record()
+
+    for s_ in range(args.warmup):
+        step(100 + s_)
+    eng.check()
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    t_steps, t_kernel = 0.0, 0.0
+    for s_ in range(args.steps):
+        flush.fill_(s_ & 0xFF)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step(1000 + s_)
+        e1.record()
+        e1.synchronize()
+        t_steps += e0.elapsed_time(e1) * 1e-3
+        t_kernel += ev_k0.elapsed_time(ev_k1) * 1e-3
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    eng.check()
+    t_max = reduce_max(t_steps, world, dev)
+    tk_max = reduce_max(t_kernel, world, dev)
+    value = attempts_per_step * args.steps * world / t_max / 1e9
+    # end to end through the public Python API: couplings built on the host, uploaded, init, rounds,
+    # energies downloaded
+    e2e_steps = max(1, min(args.steps, 3))
+    barrier(world)
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        lat2 = Lattice.edwards_anderson(3, w["L"], w["seed"])
+        e2 = MsEngine(lat2, betas, seed=7 + k, sweeps_per_round=w["spr"], instance=rank, device=dev)
+        e2.init()
+        e2.run(rounds)
+        energies = e2.best_energy.cpu().numpy()
+    t_e2e = reduce_max(time.perf_counter() - t0, world, dev)
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        launch_s = tk_max / args.steps
+        achieved = attempts_per_step * w["bytes_per_attempt"] / launch_s / 1e9
+        line = {
+            "metric": "spin-flips/ns", "value": value, "unit": "flips/ns", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32 (1 bit per spin)", "data": "synthetic",
+            "config": {"workload": w["desc"] + (f" [shortened to {rounds} rounds]" if args.rounds else ""),
+                       "rounds": rounds, "sweeps_per_round": w["spr"], "attempts_per_step": attempts_per_step,
+                       "parallelism": f"replicas-only x{world}", "l2": "flushed between steps (256 MiB write)",
+                       "best_energy_per_spin": float(energies.min()) / w["n"]},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": load_traffic("ms_run_kernel/ea3d64"), "peak_kind": peak_kind,
+                         "kernel": "ms_run_kernel", "bytes_per_attempt": w["bytes_per_attempt"],
+                         "kernel_ms": launch_s * 1e3,
+                         "note": "4 MiB of packed spins stay in L2: the HBM line is not the binding one"},
+            "e2e": {"value": attempts_per_step * e2e_steps * world / t_e2e / 1e9, "unit": "flips/ns",
+                    "h2d_bytes_per_step": int(lat.jneg.nbytes + betas.nbytes + 4 * w["R"] * 6),
+                    "d2h_bytes_per_step": int(8 * w["R"]), "api": "Lattice + MsEngine (Python over the C ABI)"},
+            "gpu_launches": 2 * args.steps,
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_ms(w, lat)
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -606,6 +730,8 @@ def main():
         bench_batched(args)
     elif args.workload == "sk512":
         bench_sk(args)
+    elif args.workload == "ea3d64":
+        bench_ms(args)
     else:
         bench_b200(args)
 
