@@ -410,6 +410,79 @@ DRIFT_PT_API int drift_pt_sk_energy(const DriftPtSkProblem* problem, int32_t n_r
                                     int64_t* energy, void* stream);
 
 /* ---------------------------------------------------------------------------------------------
+ * Tensor-core GEMM for the proposal network (no counterpart in the reference, which has no
+ * learned component): C[m][n] = epi(sum_k A[m][k] B[n][k]) with A [M][lda] and B [N][ldb] bf16,
+ * K contiguous, FP32 accumulation in tensor memory. epi: + bias[n] (optional), then ReLU (act = 1)
+ * or, when relu_ref is given, a multiply by (relu_ref[m][n] > 0) (relu_ref [M][ldc] bf16); the
+ * result is stored to out_f32 and / or out_bf16 ([M][ldc]). K, lda, ldb multiples of 8; A and B
+ * 16-byte aligned. error_flag (device int, may be NULL) is set to DRIFT_PT_ETIMEOUT if a bounded
+ * wait inside the kernel gives up.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct DriftPtGemm {
+  int32_t M, N, K, lda, ldb, ldc, act, reserved;
+  const void* A;             /* bf16 [M][lda]                                                */
+  const void* B;             /* bf16 [N][ldb]                                                */
+  const float* bias;         /* [N] or NULL                                                  */
+  const void* relu_ref;      /* bf16 [M][ldc] or NULL                                        */
+  float* out_f32;            /* [M][ldc] or NULL                                             */
+  void* out_bf16;            /* bf16 [M][ldc] or NULL                                        */
+} DriftPtGemm;
+
+DRIFT_PT_API int drift_pt_gemm_bf16(const DriftPtGemm* gemm, int32_t* error_flag, void* stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Proposal network (no counterpart in the reference): a masked autoregressive MLP over n spins,
+ * q(x) = prod_i sigma(x_i l_i(x_<i)), l = W3 relu(W2 relu(W1 x + b1) + b2) + b3, with the masks of
+ * unit degrees (input i: degree i+1; hidden degrees 1..n-1; W1[k][i] kept iff m1(k) >= i+1,
+ * W2[k'][k] iff m2(k') >= m1(k), W3[i][k'] iff i+1 > m2(k')). Training kernels (element-wise parts;
+ * the products are drift_pt_gemm_bf16):
+ * ------------------------------------------------------------------------------------------- */
+/* logq[b] = sum_i log sigma(x_i l_i); dlogits = -scale x sigma(-x l) (bf16, may be NULL). */
+DRIFT_PT_API int drift_pt_made_loss(int32_t batch, int32_t n, const float* logits, const int8_t* x, float* logq,
+                                    void* dlogits_bf16, float scale, void* stream);
+DRIFT_PT_API int drift_pt_made_spins_to_bf16(int64_t count, const int8_t* x, void* out_bf16, void* stream);
+DRIFT_PT_API int drift_pt_transpose_bf16(int32_t rows, int32_t cols, const void* in, void* out, void* stream);
+DRIFT_PT_API int drift_pt_colsum_bf16(int32_t rows, int32_t cols, const void* in, float* out, void* stream);
+/* Adam (bias-corrected, step >= 1) on a [rows][cols] fp32 tensor; entries with mask 0 are held at 0.
+ * With w_bf16 / wt_bf16 it also writes the bf16 copy and its transpose. */
+DRIFT_PT_API int drift_pt_adam(int32_t rows, int32_t cols, float* w, const float* g, float* m, float* v,
+                               const uint8_t* mask, float lr, float beta1, float beta2, float eps, int32_t step,
+                               void* w_bf16, void* wt_bf16, void* stream);
+
+typedef struct DriftPtMadeNet { /* device arrays */
+  int32_t n, h1, h2;
+  int32_t max_units_per_degree; /* <= 4                                                        */
+  const void* w1t;           /* bf16 [n][h1]  (W1 transposed, masked)                        */
+  const void* w2t;           /* bf16 [h1][h2]                                                */
+  const void* w3t;           /* bf16 [h2][n]                                                 */
+  const float* b1;           /* [h1]                                                         */
+  const float* b2;           /* [h2]                                                         */
+  const float* b3;           /* [n]                                                          */
+  const int32_t* ord1;       /* [h1] first-layer units sorted by degree                      */
+  const int32_t* off1;       /* [n+1] units of degree d at ord1[off1[d-1] .. off1[d])         */
+  const int32_t* ord2;       /* [h2]                                                         */
+  const int32_t* off2;       /* [n+1]                                                        */
+} DriftPtMadeNet;
+
+/* mode 0: draw count configurations x [count][n] (+-1) from q with Philox(i, sample, stream_id,
+ * 8 << 24; seed) and return log q of each; mode 1: log q of the given x. Both walk the spins in
+ * order and accumulate every sum in one fixed order, so the log q of a drawn x equals its
+ * mode-1 value exactly. */
+DRIFT_PT_API int drift_pt_made_sample(const DriftPtMadeNet* net, int32_t count, int32_t mode, int8_t* x,
+                                      float* logq, uint64_t seed, uint32_t stream_id, void* stream);
+
+/* Exact Metropolis-Hastings step for whole-configuration proposals on the dense layer's state:
+ * slot s (if active[s], or all when active is NULL) takes proposal x' with probability
+ * min(1, exp(-beta_rung (E' - E)) q(x) / q(x')), log of the ratio in double from the exact int64
+ * energies (units 2^-(shift+1)) and the fp32 log q values; uniform from
+ * Philox(slot, round lo, round hi, 9 << 24 | instance; seed). Counts per rung in prop_tried /
+ * prop_accepted [R]; an accepted proposal below the slot's best also becomes its best. */
+DRIFT_PT_API int drift_pt_made_mh(const DriftPtSkProblem* problem, const DriftPtSkRunArgs* args, DriftPtSkState* state,
+                                  const int8_t* proposals, const int64_t* prop_energy, const float* logq_prop,
+                                  const float* logq_cur, const uint8_t* active, int64_t* prop_tried,
+                                  int64_t* prop_accepted, int64_t round, void* stream);
+
+/* ---------------------------------------------------------------------------------------------
  * Host convenience: one call from host buffers to host results (the problem.bin -> result.bin
  * contract of cuda/ising_pt.cu:159-243 and drift/gpu.py:83-114). Allocates and frees device
  * memory internally; synchronous.
