@@ -500,6 +500,8 @@ def bench_sk(args):
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_sk(w, sk)
+        if args.ttt:
+            line["time_to_target"] = time_to_target(w, sk, args, dev)
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -618,6 +620,69 @@ def bench_ms(args):
         dist.destroy_process_group()
 
 
+def time_to_target(w, sk, args, dev):
+    """Wall time for plain PT and for neural-proposal PT (sample collection and training included)
+    to reach the best energy of a long plain-PT run, within 1e-6 relative; a few seeds, bounded."""
+    import torch
+
+    from drift_b200.made import Made
+    from drift_b200.neural import NeuralPT, collect_cold_samples
+    from drift_b200.sk import SkEngine
+
+    betas = ladder(w)
+    unit = sk.energy_unit
+    spr, chunk = w["spr"], 50
+    ref = SkEngine(sk, betas, seed=100, sweeps_per_round=spr, replicas_per_cta=args.sk_g, device=dev)
+    ref.init()
+    ref.run(args.ttt_ref_sweeps // spr)
+    ref.check()
+    target = float(ref.best_energy.min().item()) * unit
+    goal = target + 1e-6 * abs(target)
+
+    def reached(eng):
+        return float(eng.best_energy.min().item()) * unit <= goal
+
+    out = {"target_energy": target, "target_from": f"plain PT, seed 100, {args.ttt_ref_sweeps} sweeps",
+           "cap_s": args.ttt_cap_s, "plain": [], "neural": []}
+    for seed in range(1, args.ttt_seeds + 1):
+        eng = SkEngine(sk, betas, seed=seed, sweeps_per_round=spr, replicas_per_cta=args.sk_g, device=dev)
+        eng.init()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sweeps = 0
+        while not reached(eng) and time.perf_counter() - t0 < args.ttt_cap_s:
+            eng.run(chunk)
+            sweeps += chunk * spr
+        dt = time.perf_counter() - t0
+        out["plain"].append({"seed": seed, "seconds": dt, "sweeps": sweeps, "reached": reached(eng)})
+        # neural: the same start; plain rounds that collect the training set, training, then rounds
+        # with proposals at the 8 coldest rungs
+        eng = SkEngine(sk, betas, seed=seed, sweeps_per_round=spr, replicas_per_cta=args.sk_g, device=dev)
+        eng.init()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        data = collect_cold_samples(eng, args.ttt_samples, n_cold=8)
+        t_collect = time.perf_counter() - t0
+        made = Made(w["n"], (1024, 1024), seed=seed, device=dev)
+        made.train(data, epochs=args.ttt_epochs, batch=512, lr=1e-3)
+        t_train = time.perf_counter() - t0 - t_collect
+        npt = NeuralPT(sk, betas, made, n_cold=8, engine=eng)
+        rounds = 0
+        while not reached(eng) and time.perf_counter() - t0 < args.ttt_cap_s:
+            npt.run(chunk // 10)
+            rounds += chunk // 10
+        dt = time.perf_counter() - t0
+        acc = npt.acceptance()[-8:]
+        out["neural"].append({"seed": seed, "seconds": dt, "reached": reached(eng), "collect_s": t_collect,
+                              "train_s": t_train, "proposal_rounds": rounds,
+                              "proposal_acceptance_cold8": float(np.nanmean(acc)) if np.isfinite(acc).any() else None})
+    for k in ("plain", "neural"):
+        ts = [r["seconds"] for r in out[k]]
+        out[k + "_median_s"] = float(np.median(ts))
+    out["speedup_neural_over_plain"] = out["plain_median_s"] / out["neural_median_s"]
+    return out
+
+
 def bench_batched(args):
     import torch
 
@@ -720,7 +785,13 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="maxcut3reg", choices=list(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--sk-g", type=int, default=4, help="dense workload: replicas per CTA (1..12)")
+    ap.add_argument("--sk-g", type=int, default=2, help="dense workload: replicas per CTA (1..12)")
+    ap.add_argument("--ttt", action="store_true", help="dense workload: add time-to-target, neural vs plain PT")
+    ap.add_argument("--ttt-seeds", type=int, default=3)
+    ap.add_argument("--ttt-cap-s", type=float, default=20.0)
+    ap.add_argument("--ttt-ref-sweeps", type=int, default=100000)
+    ap.add_argument("--ttt-samples", type=int, default=100000)
+    ap.add_argument("--ttt-epochs", type=int, default=5)
     ap.add_argument("--rounds", type=int, default=0,
                     help="override the rounds per step (profiling of a short case; the line then says so)")
     args = ap.parse_args()

@@ -134,80 +134,173 @@ struct MadeArgs {
   uint32_t k0, k1, stream;
 };
 
-template <int S>
+// Thread t owns first-layer units t, t+T, ... (kH1 of them), second-layer units likewise (kH2) and
+// logits likewise (kN): their partial sums for the S samples of the CTA live in its registers. It
+// also holds its slices of the next step's weights, loaded one step ahead. Shared memory carries
+// only what crosses threads in a step: the finished units' ReLU values, the next logit and the
+// drawn spins.
+template <int S, int kH1, int kH2, int kN>
 __global__ void __launch_bounds__(256) made_sample_kernel(const MadeArgs a) {
-  extern __shared__ __align__(16) unsigned char m_raw[];
+  __shared__ float r1[4][S], r2[4][S], lnext[S];
+  __shared__ float xs[S];
+  extern __shared__ int m_idx[];  // the degree orders: off1 [n+1], off2 [n+1], ord1 [H1], ord2 [H2]
   const int n = a.n, H1 = a.h1, H2 = a.h2;
-  float* h1p = reinterpret_cast<float*>(m_raw);  // [S][H1]
-  float* h2p = h1p + (size_t)S * H1;              // [S][H2]
-  float* outp = h2p + (size_t)S * H2;             // [S][n]
-  float* r1 = outp + (size_t)S * n;               // [S][4] finished first-layer values of this step
-  float* r2 = r1 + 4 * S;                         // [S][4]
-  int8_t* xs = reinterpret_cast<int8_t*>(r2 + 4 * S);  // [S] this step's spins
   const int tid = threadIdx.x, T = blockDim.x;
+  int* off1 = m_idx;
+  int* off2 = off1 + (n + 1);
+  int* ord1 = off2 + (n + 1);
+  int* ord2 = ord1 + H1;
+  for (int k = tid; k <= n; k += T) {
+    off1[k] = a.off1[k];
+    off2[k] = a.off2[k];
+  }
+  for (int k = tid; k < H1; k += T) ord1[k] = a.ord1[k];
+  for (int k = tid; k < H2; k += T) ord2[k] = a.ord2[k];
+  __syncthreads();
   const int base = blockIdx.x * S;
   const int ns = min(S, a.count - base);
-  for (int idx = tid; idx < S * H1; idx += T) h1p[idx] = a.b1[idx % H1];
-  for (int idx = tid; idx < S * H2; idx += T) h2p[idx] = a.b2[idx % H2];
-  for (int idx = tid; idx < S * n; idx += T) outp[idx] = a.b3[idx % n];
+  float h1[kH1][S], h2[kH2][S], lo[kN][S];
+#pragma unroll
+  for (int j = 0; j < kH1; ++j) {
+    const float bv = tid + j * T < H1 ? a.b1[tid + j * T] : 0.0f;
+#pragma unroll
+    for (int s = 0; s < S; ++s) h1[j][s] = bv;
+  }
+#pragma unroll
+  for (int j = 0; j < kH2; ++j) {
+    const float bv = tid + j * T < H2 ? a.b2[tid + j * T] : 0.0f;
+#pragma unroll
+    for (int s = 0; s < S; ++s) h2[j][s] = bv;
+  }
+#pragma unroll
+  for (int j = 0; j < kN; ++j) {
+    const float bv = tid + j * T < n ? a.b3[tid + j * T] : 0.0f;
+#pragma unroll
+    for (int s = 0; s < S; ++s) lo[j][s] = bv;
+  }
+  // weight slices of a step: column i of W1, rows of W2 for the finishing first-layer units and rows
+  // of W3 for the finishing second-layer units (at most 4 of each)
+  float w1[kH1], w2[4][kH2], w3[4][kN];
+  auto fetch = [&](int i, float (&v1)[kH1], float (&v2)[4][kH2], float (&v3)[4][kN]) {
+    const __nv_bfloat16* col = a.w1t + (size_t)i * H1;
+#pragma unroll
+    for (int j = 0; j < kH1; ++j) v1[j] = tid + j * T < H1 ? __bfloat162float(col[tid + j * T]) : 0.0f;
+    const int f1a = off1[i], nf1 = off1[i + 1] - f1a;
+    const int f2a = off2[i], nf2 = off2[i + 1] - f2a;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const __nv_bfloat16* row2 = u < nf1 ? a.w2t + (size_t)ord1[f1a + u] * H2 : nullptr;
+      const __nv_bfloat16* row3 = u < nf2 ? a.w3t + (size_t)ord2[f2a + u] * n : nullptr;
+#pragma unroll
+      for (int j = 0; j < kH2; ++j) v2[u][j] = row2 && tid + j * T < H2 ? __bfloat162float(row2[tid + j * T]) : 0.0f;
+#pragma unroll
+      for (int j = 0; j < kN; ++j) v3[u][j] = row3 && tid + j * T < n ? __bfloat162float(row3[tid + j * T]) : 0.0f;
+    }
+  };
+  fetch(0, w1, w2, w3);
+  // l_0 is b3[0]
+  if (tid == 0)
+#pragma unroll
+    for (int s = 0; s < S; ++s) lnext[s] = lo[0][s];
   float lq = 0.0f;  // thread s < ns accumulates sample s
   __syncthreads();
   for (int i = 0; i < n; ++i) {
     // x_i from l_i (final: every second-layer unit of degree <= i is in)
     if (tid < ns) {
-      const float l = outp[tid * n + i];
-      int8_t s;
+      const float l = lnext[tid];
+      float sv;
       if (a.mode == 0) {
         const U4 u = philox(U4{(uint32_t)i, (uint32_t)(base + tid), a.stream, ctr3(kTagMadeSample, 0)}, a.k0, a.k1);
         const float uf = (float)(u.x >> 8) * 0x1.0p-24f;
-        s = uf < 1.0f / (1.0f + expf(-l)) ? (int8_t)1 : (int8_t)-1;
-        a.x[(size_t)(base + tid) * n + i] = s;
+        sv = uf < 1.0f / (1.0f + expf(-l)) ? 1.0f : -1.0f;
+        a.x[(size_t)(base + tid) * n + i] = (int8_t)sv;
       } else {
-        s = a.x[(size_t)(base + tid) * n + i];
+        sv = (float)a.x[(size_t)(base + tid) * n + i];
       }
-      xs[tid] = s;
-      lq += log_sigmoid((float)s * l);
+      xs[tid] = sv;
+      lq += log_sigmoid(sv * l);
     }
+    // the next step's weights, in flight during this step
+    float nw1[kH1], nw2[4][kH2], nw3[4][kN];
+    if (i + 1 < n) fetch(i + 1, nw1, nw2, nw3);
+    const int f1a = off1[i], nf1 = off1[i + 1] - f1a;
+    const int f2a = off2[i], nf2 = off2[i + 1] - f2a;
     __syncthreads();
-    // first layer: += column i of W1 (zero where the mask excludes it)
+    // first layer: += column i of W1 (zero where masked); owners of finishing units publish ReLU
     {
-      const __nv_bfloat16* col = a.w1t + (size_t)i * H1;
-      for (int k = tid; k < H1; k += T) {
-        const float wv = __bfloat162float(col[k]);
-        if (wv != 0.0f)
-          for (int s = 0; s < ns; ++s) h1p[s * H1 + k] += wv * (float)xs[s];
+      float xv[S];
+#pragma unroll
+      for (int s = 0; s < S; ++s) xv[s] = xs[s];
+#pragma unroll
+      for (int j = 0; j < kH1; ++j)
+#pragma unroll
+        for (int s = 0; s < S; ++s) h1[j][s] += w1[j] * xv[s];
+    }
+    for (int u = 0; u < nf1; ++u) {
+      const int k = ord1[f1a + u];
+      if (k % T == tid) {
+        const int jj = k / T;
+#pragma unroll
+        for (int j = 0; j < kH1; ++j)
+          if (j == jj)
+#pragma unroll
+            for (int s = 0; s < S; ++s) r1[u][s] = fmaxf(h1[j][s], 0.0f);
       }
     }
     __syncthreads();
-    // first-layer units of degree i+1 are finished: their ReLU feeds the second layer
-    const int f1a = a.off1[i], f1b = a.off1[i + 1];
-    for (int idx = tid; idx < (f1b - f1a) * ns; idx += T) {
-      const int u = idx / ns, s = idx % ns;
-      r1[s * 4 + u] = fmaxf(h1p[s * H1 + a.ord1[f1a + u]], 0.0f);
+    // second layer: += finishing first-layer units; owners of finishing second-layer units publish
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (u >= nf1) break;
+      float rv[S];
+#pragma unroll
+      for (int s = 0; s < S; ++s) rv[s] = r1[u][s];
+#pragma unroll
+      for (int j = 0; j < kH2; ++j)
+#pragma unroll
+        for (int s = 0; s < S; ++s) h2[j][s] += w2[u][j] * rv[s];
     }
-    __syncthreads();
-    for (int u = 0; u < f1b - f1a; ++u) {
-      const __nv_bfloat16* row = a.w2t + (size_t)a.ord1[f1a + u] * H2;
-      for (int k = tid; k < H2; k += T) {
-        const float wv = __bfloat162float(row[k]);
-        if (wv != 0.0f)
-          for (int s = 0; s < ns; ++s) h2p[s * H2 + k] += wv * r1[s * 4 + u];
+    for (int u = 0; u < nf2; ++u) {
+      const int k = ord2[f2a + u];
+      if (k % T == tid) {
+        const int jj = k / T;
+#pragma unroll
+        for (int j = 0; j < kH2; ++j)
+          if (j == jj)
+#pragma unroll
+            for (int s = 0; s < S; ++s) r2[u][s] = fmaxf(h2[j][s], 0.0f);
       }
     }
     __syncthreads();
-    // second-layer units of degree i+1 are finished: their ReLU feeds the logits
-    const int f2a = a.off2[i], f2b = a.off2[i + 1];
-    for (int idx = tid; idx < (f2b - f2a) * ns; idx += T) {
-      const int u = idx / ns, s = idx % ns;
-      r2[s * 4 + u] = fmaxf(h2p[s * H2 + a.ord2[f2a + u]], 0.0f);
+    // logits: += finishing second-layer units; the owner of l_{i+1} publishes it
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (u >= nf2) break;
+      float rv[S];
+#pragma unroll
+      for (int s = 0; s < S; ++s) rv[s] = r2[u][s];
+#pragma unroll
+      for (int j = 0; j < kN; ++j)
+#pragma unroll
+        for (int s = 0; s < S; ++s) lo[j][s] += w3[u][j] * rv[s];
     }
-    __syncthreads();
-    for (int u = 0; u < f2b - f2a; ++u) {
-      const __nv_bfloat16* row = a.w3t + (size_t)a.ord2[f2a + u] * n;
-      for (int k = tid; k < n; k += T) {
-        const float wv = __bfloat162float(row[k]);
-        if (wv != 0.0f)
-          for (int s = 0; s < ns; ++s) outp[s * n + k] += wv * r2[s * 4 + u];
+    if (i + 1 < n && (i + 1) % T == tid) {
+      const int jj = (i + 1) / T;
+#pragma unroll
+      for (int j = 0; j < kN; ++j)
+        if (j == jj)
+#pragma unroll
+          for (int s = 0; s < S; ++s) lnext[s] = lo[j][s];
+    }
+    if (i + 1 < n) {
+#pragma unroll
+      for (int j = 0; j < kH1; ++j) w1[j] = nw1[j];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+#pragma unroll
+        for (int j = 0; j < kH2; ++j) w2[u][j] = nw2[u][j];
+#pragma unroll
+        for (int j = 0; j < kN; ++j) w3[u][j] = nw3[u][j];
       }
     }
     __syncthreads();
@@ -348,14 +441,17 @@ extern "C" int drift_pt_made_sample(const DriftPtMadeNet* net, int32_t count, in
   a.k0 = (uint32_t)(seed & 0xffffffffu);
   a.k1 = (uint32_t)(seed >> 32);
   a.stream = stream_id;
-  constexpr int S = 8;
+  constexpr int S = 8, T = 256;
   a.S = S;
-  const size_t smem = (size_t)S * (a.h1 + a.h2 + a.n) * 4 + 8 * S * 4 + 16;
+  // per-thread weight slices: up to 4 first-layer, 4 second-layer and 2 logit entries per unit
+  if (a.h1 > 4 * T || a.h2 > 4 * T || a.n > 2 * T)
+    return set_error(DRIFT_PT_EUNSUPPORTED, "made_sample: hidden widths up to %d and n up to %d", 4 * T, 2 * T);
+  auto fn = made_sample_kernel<S, 4, 4, 2>;
+  const size_t smem = (size_t)(2 * (a.n + 1) + a.h1 + a.h2) * sizeof(int);
   int per_sm = 0;
-  int rc = prepare_kernel((const void*)made_sample_kernel<S>, 256, smem, &per_sm);
+  int rc = prepare_kernel((const void*)fn, T, smem, &per_sm);
   if (rc) return rc;
-  if (per_sm < 1) return set_error(DRIFT_PT_EUNSUPPORTED, "made_sample: network too wide for shared memory");
-  made_sample_kernel<S><<<(count + S - 1) / S, 256, smem, static_cast<cudaStream_t>(stream)>>>(a);
+  fn<<<(count + S - 1) / S, T, smem, static_cast<cudaStream_t>(stream)>>>(a);
   return made_fail("made_sample_kernel");
 }
 

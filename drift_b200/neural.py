@@ -52,9 +52,11 @@ class NeuralPT:
     proposal per replica at the n_cold coldest rungs)."""
 
     def __init__(self, model: SkModel, betas, made: Made, *, seed: int = 0, sweeps_per_round: int = 10,
-                 n_cold: int = 8, replicas_per_cta: int = 0, instance: int = 0, device="cuda"):
-        self.eng = SkEngine(model, betas, seed=seed, sweeps_per_round=sweeps_per_round, instance=instance,
-                            replicas_per_cta=replicas_per_cta, device=device)
+                 n_cold: int = 8, replicas_per_cta: int = 0, instance: int = 0, device="cuda",
+                 engine: SkEngine | None = None):
+        # `engine`: continue an existing plain-PT run (e.g. the one whose samples trained `made`)
+        self.eng = engine or SkEngine(model, betas, seed=seed, sweeps_per_round=sweeps_per_round, instance=instance,
+                                      replicas_per_cta=replicas_per_cta, device=device)
         self.made = made
         self.n_cold = n_cold
         torch = self.torch = self.eng.torch
