@@ -137,3 +137,16 @@ def sk_model(n: int, seed: int) -> IsingModel:
     J[iu, ju] = v
     J[ju, iu] = v
     return IsingModel(J, np.zeros(n))
+
+
+def gnp_pm(n: int, p: float, seed: int, field: int = 0) -> IsingModel:
+    """G(n, p) with +-1 couplings: the edges of random_graph(n, p, seed), a sign per edge in row-major
+    edge order from default_rng(seed + 1); with `field`, h_i = +-field from default_rng(seed + 2)."""
+    A = random_graph(n, p, seed)
+    iu, ju = np.nonzero(np.triu(A, 1))
+    signs = np.random.default_rng(seed + 1).integers(0, 2, size=iu.size) * 2.0 - 1.0
+    J = np.zeros((n, n))
+    J[iu, ju] = signs
+    J[ju, iu] = signs
+    h = np.zeros(n) if not field else (np.random.default_rng(seed + 2).integers(0, 2, size=n) * 2.0 - 1.0) * field
+    return IsingModel(J, h)

@@ -24,9 +24,10 @@ def geometric_ladder(n_replicas: int, T_min: float, T_max: float) -> np.ndarray:
 
 
 def parallel_tempering(model, *, n_replicas=16, T_min=0.1, T_max=5.0, n_rounds=300, sweeps_per_round=5, seed=0,
-                       record=False):
+                       record=False, record_spins=False):
     """drift/solvers/parallel_tempering.py:52-124. Returns a dict; with ``record`` also the
-    per-round rung energies (n_rounds, R) and |m| (n_rounds, R) after the sweeps."""
+    per-round rung energies (n_rounds, R) and |m| (n_rounds, R) after the sweeps; with
+    ``record_spins`` the rung configurations (n_rounds, R, n) at the same points."""
     rng = np.random.default_rng(seed)
     n = model.n
     R = n_replicas
@@ -40,6 +41,7 @@ def parallel_tempering(model, *, n_replicas=16, T_min=0.1, T_max=5.0, n_rounds=3
     best_history = np.empty(n_rounds, dtype=np.float64)
     rec_E = np.empty((n_rounds, R)) if record else None
     rec_m = np.empty((n_rounds, R)) if record else None
+    rec_s = np.empty((n_rounds, R, n), np.int8) if record_spins else None
     swaps_tried = 0
     swaps_done = 0
     J, h = model.J, model.h
@@ -61,6 +63,8 @@ def parallel_tempering(model, *, n_replicas=16, T_min=0.1, T_max=5.0, n_rounds=3
         if record:
             rec_E[rnd] = E
             rec_m[rnd] = np.abs(s.mean(axis=1))
+        if record_spins:
+            rec_s[rnd] = s.astype(np.int8)
         start = rnd % 2
         for r in range(start, R - 1, 2):
             swaps_tried += 1
@@ -81,4 +85,6 @@ def parallel_tempering(model, *, n_replicas=16, T_min=0.1, T_max=5.0, n_rounds=3
     if record:
         out["rung_energy"] = rec_E
         out["rung_absm"] = rec_m
+    if record_spins:
+        out["rung_spins"] = rec_s
     return out
