@@ -243,6 +243,55 @@ def bench_reference(args):
     }), flush=True)
 
 
+def bench_reference_gpu(args):
+    """The reference's own GPU engine (cuda/ising_pt.cu compiled unchanged for sm_100a into
+    oracle/_ref by oracle/Makefile) on the workload's problem file, as drift/gpu.py runs it."""
+    rank, world, local = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    import tempfile
+
+    import oracle
+    from drift_b200.problem_io import parse_stderr, read_result, write_problem
+
+    w = WORKLOADS[args.workload]
+    if not os.path.exists(oracle.REF_BIN) or args.workload not in ("maxcut3reg", "ea2d", "sk512"):
+        why = "oracle/_ref/ising_pt not built" if not os.path.exists(oracle.REF_BIN) else \
+            "the reference engine runs one instance of a CSR model (no batched or bit-packed input)"
+        print(json.dumps({"impl": "reference-gpu", "unavailable": why}), flush=True)
+        return
+    model = make_model(args.workload)
+    b = ladder(w)
+    # the reference's per-attempt loop is O(degree); the dense SK model runs a shortened job
+    rounds = args.rounds or (200 if args.workload == "sk512" else w["sweeps"] // w["spr"])
+    vals, walls, bests = [], [], []
+    with tempfile.TemporaryDirectory() as d:
+        prob, res = os.path.join(d, "problem.bin"), os.path.join(d, "result.bin")
+        for s_ in range(args.warmup + args.steps):
+            write_problem(prob, model, n_replicas=w["R"], T_min=1.0 / b[-1], T_max=1.0 / b[0], n_rounds=rounds,
+                          sweeps_per_round=w["spr"], seed=1000 + s_)
+            t0 = time.perf_counter()
+            r = subprocess.run([oracle.REF_BIN, prob, res], capture_output=True, text=True, timeout=1800)
+            wall = time.perf_counter() - t0
+            if r.returncode != 0:
+                print(json.dumps({"impl": "reference-gpu", "unavailable": f"reference engine failed: {r.stderr[-300:]}"}))
+                return
+            if s_ >= args.warmup:
+                f = parse_stderr(r.stderr)
+                vals.append(f["throughput"] / 1e9)
+                walls.append(float(w["R"]) * rounds * w["spr"] * w["n"] / wall / 1e9)
+                bests.append(read_result(res, w["n"])[0])
+    print(json.dumps({
+        "impl": "reference-gpu", "metric": "spin-flips/ns", "value": float(np.median(vals)), "unit": "flips/ns",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64 field, f32 spins",
+        "data": "synthetic",
+        "config": {"workload": w["desc"], "rounds": rounds, "sweeps_per_round": w["spr"],
+                   "timer": "the reference's own (round loop, device-synchronised)"},
+        "wall_clock_flips_per_ns": float(np.median(walls)), "best_energy": float(np.min(bests)),
+        "binary": "oracle/_ref/ising_pt: cuda/ising_pt.cu compiled unchanged with -gencode arch=compute_100a,code=sm_100a",
+    }), flush=True)
+
+
 def cpu_baseline_oracle(w, model_name, budget_s=12.0):
     """The C oracle (OpenMP over replicas) on the host cores: a bounded number of rounds."""
     import oracle
@@ -782,7 +831,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference", "reference-gpu"])
     ap.add_argument("--workload", default="maxcut3reg", choices=list(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sk-g", type=int, default=2, help="dense workload: replicas per CTA (1..12)")
@@ -797,6 +846,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         bench_reference(args)
+    elif args.impl == "reference-gpu":
+        bench_reference_gpu(args)
     elif args.workload == "batched_er":
         bench_batched(args)
     elif args.workload == "sk512":

@@ -36,6 +36,29 @@ def _stale(out: str, deps: list[str]) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+CLI_PATH = os.path.join(HERE, "ising_pt")
+
+
+def build_cli(force: bool = False, verbose: bool = False) -> str:
+    """The `ising_pt` command-line twin of the reference executable, linked against libdrift_pt.so."""
+    src = os.path.join(CSRC, "ising_pt_cli.cpp")
+    deps = [src, LIB_PATH, os.path.join(os.path.dirname(HERE), "include", "drift_pt.h")]
+    if not force and not _stale(CLI_PATH, deps):
+        return CLI_PATH
+    cxx = shutil.which("g++") or shutil.which("c++")
+    if cxx is None:
+        raise RuntimeError("a C++ compiler is required to build the ising_pt command")
+    cmd = [cxx, "-O2", "-std=c++17", "-o", CLI_PATH + ".tmp", src, "-L" + HERE, "-ldrift_pt",
+           "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"building ising_pt failed ({r.returncode}):\n{r.stdout}\n{r.stderr}")
+    os.replace(CLI_PATH + ".tmp", CLI_PATH)
+    return CLI_PATH
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
     deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
@@ -57,3 +80,4 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose=True))
+    print(build_cli(force="--force" in sys.argv, verbose=True))

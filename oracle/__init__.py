@@ -50,6 +50,22 @@ def build(force: bool = False) -> str:
     return LIB_PATH
 
 
+REF_BIN = os.path.join(HERE, "_ref", "ising_pt")
+REFERENCE_TREE = "/root/reference"
+
+
+def build_ref() -> str | None:
+    """Compile the reference's own GPU engine (cuda/ising_pt.cu, unchanged) into _ref/ when its
+    source tree is present; returns the binary's path if it exists afterwards."""
+    src = os.path.join(REFERENCE_TREE, "cuda", "ising_pt.cu")
+    if os.path.exists(src):
+        r = subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE={REFERENCE_TREE}"], capture_output=True,
+                           text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"reference GPU engine build failed:\n{r.stdout}\n{r.stderr}")
+    return REF_BIN if os.path.exists(REF_BIN) else None
+
+
 class _Problem(C.Structure):
     _fields_ = [("n", C.c_int32), ("row_ptr", C.c_void_p), ("col_idx", C.c_void_p), ("weight", C.c_void_p),
                 ("h", C.c_void_p), ("n_colors", C.c_int32), ("color_ptr", C.c_void_p), ("color_spins", C.c_void_p),
