@@ -1,7 +1,8 @@
 """Benchmark: spin-flip attempts per ns of the B200 parallel-tempering engine.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload maxcut3reg|ea2d|batched_er|ea3d64|sk512]
-                    [--impl b200|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W]
+                    [--workload maxcut3reg|ea2d|batched_er|ea3d64|maxcut3reg_r2048|sk512]
+                    [--impl b200|reference|reference-gpu]
 
 Workload (default ``maxcut3reg``): plain PT on MaxCut as Ising over a random 3-regular graph,
 N = 4096 (seeded), J = -1 on edges, h = 0, int8 spins, greedy colouring (4 colours), 64 replicas
@@ -47,9 +48,6 @@ WORKLOADS = {
                             "beta 0.1-3.0; 500 of the job's 5e4 sweeps per step",
                        n_instances=512, seed=3, R=32, beta=(0.1, 3.0), sweeps=500, spr=5,
                        bytes_per_attempt=2.0 + 6 * 8 / 32 + 4 / 32),
-    # dense SK: J_ij ~ N(0, 1)/sqrt(N) (fp32 values) on the upper triangle, mirrored, h = 0, seed 4;
-    # 64 replicas, beta 0.3-3.0, rounds of 10 sweeps; 1e4 sweeps per step. Tensor-core field
-    # updates: the algorithmic work of an attempt is the 2N flops of J_i . s (drift/ising.py:68)
     # 3-D Edwards-Anderson +-J, L = 64 periodic (N = 262,144), seed 5; 128 replicas packed 32 per
     # word; beta 0.2-2.0; 1e4 sweeps in rounds of 10. Algorithmic bytes per attempt: spin read and
     # write (2 bits) + 3 coupling bits per site shared by the 128 replicas = 0.253 B
@@ -57,6 +55,15 @@ WORKLOADS = {
                         "in rounds of 10",
                    n=64 ** 3, L=64, seed=5, R=128, beta=(0.2, 2.0), sweeps=10000, spr=10,
                    bytes_per_attempt=2 / 8 + 3 / 8 / 128),
+    # the MaxCut instance above with 2048 replicas, 32 per word, on the graph multispin engine
+    # (clusters of CTAs per word chosen by the engine); 2e4 sweeps in rounds of 4 per step.
+    # Algorithmic bytes per attempt: spin read and write (2 bits) + 3 neighbour bits = 5/8 B
+    "maxcut3reg_r2048": dict(desc="MaxCut random 3-regular N=4096 (J=-1), 2048 replicas (bit-packed), beta 0.2-4.0, "
+                                  "2e4 sweeps in rounds of 4",
+                             n=4096, seed=2, R=2048, beta=(0.2, 4.0), sweeps=20000, spr=4, bytes_per_attempt=5 / 8),
+    # dense SK: J_ij ~ N(0, 1)/sqrt(N) (fp32 values) on the upper triangle, mirrored, h = 0, seed 4;
+    # 64 replicas, beta 0.3-3.0, rounds of 10 sweeps; 1e4 sweeps per step. Tensor-core field
+    # updates: the algorithmic work of an attempt is the 2N flops of J_i . s (drift/ising.py:68)
     "sk512": dict(desc="SK N=512, J~N(0,1/N) fp32, 64 replicas, beta 0.3-3.0, 1e4 sweeps in rounds of 10",
                   n=512, seed=4, R=64, beta=(0.3, 3.0), sweeps=10000, spr=10, flops_per_attempt=2 * 512),
 }
@@ -76,7 +83,7 @@ def make_model(name):
     w = WORKLOADS[name]
     if name == "sk512":
         return sk_model(w["n"], w["seed"])
-    return maxcut_3regular(w["n"], w["seed"]) if name == "maxcut3reg" else ea_2d(16, w["seed"])
+    return maxcut_3regular(w["n"], w["seed"]) if name.startswith("maxcut3reg") else ea_2d(16, w["seed"])
 
 
 def ladder(w):
@@ -190,6 +197,9 @@ def barrier(world: int):
 
 # ---------------------------------------------------------------------------------------------
 
+REF_SAMPLE_RUNGS = 64
+
+
 def run_reference_sample(args_tuple):
     """One process: the reference CPU algorithm on a bounded sample (1 round x 1 sweep of all rungs)."""
     name, seed = args_tuple
@@ -202,8 +212,10 @@ def run_reference_sample(args_tuple):
     model = model.to_dense() if hasattr(model, "to_dense") else model
     b = ladder(w)
     t0 = time.perf_counter()
-    out = ref_pt.parallel_tempering(model, n_replicas=w["R"], T_min=1.0 / b[0], T_max=1.0 / b[-1], n_rounds=1,
-                                    sweeps_per_round=1, seed=seed)
+    # the reference's cost is linear in rungs: wide ladders are sampled with REF_SAMPLE_RUNGS rungs over the
+    # same temperature range
+    out = ref_pt.parallel_tempering(model, n_replicas=min(w["R"], REF_SAMPLE_RUNGS), T_min=1.0 / b[0],
+                                    T_max=1.0 / b[-1], n_rounds=1, sweeps_per_round=1, seed=seed)
     return out["attempts"], time.perf_counter() - t0
 
 
@@ -235,10 +247,11 @@ def bench_reference(args):
         "impl": "reference", "metric": "spin-flips/ns", "value": v, "unit": "flips/ns", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": w["desc"], "sample": f"{cores} processes x (1 round x 1 sweep x {w['R']} rungs x {w['n']} spins) per step"},
+        "config": {"workload": w["desc"], "sample": f"{cores} processes x (1 round x 1 sweep x "
+                   f"{min(w['R'], REF_SAMPLE_RUNGS)} rungs x {w['n']} spins) per step"},
         "cpu_baseline": {"value": v, "unit": "flips/ns", "cores": cores, "kind": "port",
                          "sample": f"oracle/ref_pt.py (reference CPU PT restated, same NumPy stream), one process per core, "
-                                   f"{cores} x {w['R'] * w['n']:.0f} attempts per step"},
+                                   f"{cores} x {min(w['R'], REF_SAMPLE_RUNGS) * w['n']:.0f} attempts per step"},
         "e2e": {"value": v, "unit": "flips/ns", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -669,6 +682,123 @@ def bench_ms(args):
         dist.destroy_process_group()
 
 
+def cpu_baseline_gms(w, lay, budget_s=12.0):
+    """The graph multispin oracle (scalar, one replica bit at a time) on a bounded number of rounds."""
+    import oracle
+
+    b = ladder(w)
+    t0 = time.perf_counter()
+    st = oracle.gms_run(lay, b, n_rounds=1, sweeps_per_round=1, seed=3)
+    sweeps = 1
+    while time.perf_counter() - t0 < budget_s:
+        st = oracle.gms_run(lay, b, n_rounds=1, sweeps_per_round=1, seed=3, state=st, round_offset=sweeps)
+        sweeps += 1
+    dt = time.perf_counter() - t0
+    attempts = sweeps * w["R"] * w["n"]
+    return {"value": attempts / dt / 1e9, "unit": "flips/ns", "cores": 1, "kind": "port",
+            "sample": f"oracle/gms_oracle.c (scalar, one replica bit at a time), {sweeps} sweeps x {w['R']} replicas x "
+                      f"{w['n']} spins incl. initialisation ({attempts:.3g} attempts, {dt:.1f} s)"}
+
+
+def bench_gms(args):
+    import torch
+
+    from drift_b200.gms import GmsEngine, GmsLayout
+    from drift_b200.instances import maxcut_3regular
+
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    w = WORKLOADS[args.workload]
+    model = maxcut_3regular(w["n"], w["seed"])
+    lay = GmsLayout.from_model(model)
+    betas = ladder(w)
+    rounds = args.rounds or w["sweeps"] // w["spr"]
+    eng = GmsEngine(lay, betas, seed=1, sweeps_per_round=w["spr"], instance=rank, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    attempts_per_step = float(w["R"]) * rounds * w["spr"] * w["n"]
+    ev_k0, ev_k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def step(seed):
+        eng.seed = seed
+        eng.init()
+        ev_k0.record()
+        eng.run(rounds)
+        ev_k1.record()
+
+    for s_ in range(args.warmup):
+        step(100 + s_)
+    eng.check()
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    t_steps, t_kernel = 0.0, 0.0
+    for s_ in range(args.steps):
+        flush.fill_(s_ & 0xFF)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step(1000 + s_)
+        e1.record()
+        e1.synchronize()
+        t_steps += e0.elapsed_time(e1) * 1e-3
+        t_kernel += ev_k0.elapsed_time(ev_k1) * 1e-3
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    eng.check()
+    t_max = reduce_max(t_steps, world, dev)
+    tk_max = reduce_max(t_kernel, world, dev)
+    value = attempts_per_step * args.steps * world / t_max / 1e9
+    # end to end through the public Python API: layout built on the host from the model, uploaded,
+    # init, rounds, best energies downloaded
+    e2e_steps = max(1, min(args.steps, 3))
+    barrier(world)
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        lay2 = GmsLayout.from_model(model)
+        e2 = GmsEngine(lay2, betas, seed=7 + k, sweeps_per_round=w["spr"], instance=rank, device=dev)
+        e2.init()
+        e2.run(rounds)
+        energies = e2.best_energy.cpu().numpy()
+    t_e2e = reduce_max(time.perf_counter() - t0, world, dev)
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        launch_s = tk_max / args.steps
+        achieved = attempts_per_step * w["bytes_per_attempt"] / launch_s / 1e9
+        h2d = lay.color_ptr.nbytes + lay.ell_nbr.nbytes + lay.degree.nbytes + lay.jneg.nbytes + betas.nbytes
+        # the engine's automatic shape: one CTA per word from 16 words up, else a cluster of CTAs per word
+        kname = "gms_run_kernel" if w["R"] // 32 >= 16 else "gmc_run_kernel"
+        line = {
+            "metric": "spin-flips/ns", "value": value, "unit": "flips/ns", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32 (1 bit per spin)", "data": "synthetic",
+            "config": {"workload": w["desc"] + (f" [shortened to {rounds} rounds]" if args.rounds else ""),
+                       "rounds": rounds, "sweeps_per_round": w["spr"], "attempts_per_step": attempts_per_step,
+                       "parallelism": f"replicas-only x{world}", "l2": "flushed between steps (256 MiB write)",
+                       "engine": "graph multispin (drift_pt_gms_run)",
+                       "best_energy_per_spin": float(energies.min()) / w["n"]},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": load_traffic(f"{kname}/{args.workload}"), "peak_kind": peak_kind,
+                         "kernel": kname, "bytes_per_attempt": w["bytes_per_attempt"],
+                         "kernel_ms": launch_s * 1e3,
+                         "note": "the packed words live in shared memory for the whole launch: the HBM line is "
+                                 "not the binding one (the phases are latency-bound)"},
+            "e2e": {"value": attempts_per_step * e2e_steps * world / t_e2e / 1e9, "unit": "flips/ns",
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(8 * w["R"]),
+                    "api": "GmsLayout + GmsEngine (Python over the C ABI)"},
+            "gpu_launches": 2 * args.steps,
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_gms(w, lay)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
 def time_to_target(w, sk, args, dev):
     """Wall time for plain PT and for neural-proposal PT (sample collection and training included)
     to reach the best energy of a long plain-PT run, within 1e-6 relative; a few seeds, bounded."""
@@ -854,6 +984,8 @@ def main():
         bench_sk(args)
     elif args.workload == "ea3d64":
         bench_ms(args)
+    elif args.workload == "maxcut3reg_r2048":
+        bench_gms(args)
     else:
         bench_b200(args)
 

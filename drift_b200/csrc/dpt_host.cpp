@@ -93,6 +93,10 @@ namespace {
 
 bool is_int_in(float v, float lim) { return std::nearbyint(v) == v && std::fabs(v) <= lim; }
 
+}  // namespace
+
+namespace dpt {
+
 int validate_csr(const DriftPtCsr* c) {
   if (!c) return set_error(DRIFT_PT_EINVAL, "csr is NULL");
   if (c->n < 1) return set_error(DRIFT_PT_EINVAL, "n must be >= 1 (got %d)", c->n);
@@ -131,7 +135,7 @@ int validate_csr(const DriftPtCsr* c) {
   return DRIFT_PT_OK;
 }
 
-}  // namespace
+}  // namespace dpt
 
 extern "C" int drift_pt_layout_query(const DriftPtCsr* csr, DriftPtLayoutInfo* info) {
   clear_error();

@@ -3,6 +3,8 @@
 #include <cstdarg>
 #include <cstdint>
 
+struct DriftPtCsr;
+
 namespace dpt {
 
 // Sliced-ELL geometry: a thread owns a group of 8 consecutive positions, a warp 32 groups,
@@ -19,5 +21,9 @@ void clear_error();
 // of `threads` threads fit an SM. Results are cached per (kernel, threads, smem), so repeated
 // launches (and launches inside a stream capture) make no further attribute or occupancy calls.
 int prepare_kernel(const void* fn, int threads, size_t smem, int* per_sm);
+
+// Checks a CSR problem and its colouring (ranges, permutation, no coupling inside a colour class);
+// sets the error message and returns its status on failure.
+int validate_csr(const DriftPtCsr* csr);
 
 }  // namespace dpt

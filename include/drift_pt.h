@@ -336,6 +336,91 @@ DRIFT_PT_API int drift_pt_ms_run(const DriftPtLattice* lat, const DriftPtMsRunAr
                                  void* workspace, size_t workspace_bytes, void* stream);
 
 /* ---------------------------------------------------------------------------------------------
+ * Graph multispin layer: +-1 couplings on any graph (max degree <= 7, no field), 32 replicas per
+ * 32-bit word, one CTA (or a cluster of 2..16 CTAs) per word. No counterpart in the reference (its engine stores one float per
+ * spin per replica, cuda/ising_pt.cu:190-191); the chain is the sparse layer's colour-ordered sweep
+ * with a different uniform per attempt:
+ *   positions: the colour order of drift_pt_color_order (class c = positions color_ptr[c] ..);
+ *   bit b of word w at position p = replica slot 32w + b, 1 = spin -1;
+ *   ell_nbr[d][p] (d < degree[p]): neighbour positions; jneg[p] bit d set when that bond's J = -1;
+ *   a flip with k unsatisfied bonds has dE = 2 (deg - 2k); accepted when deg - 2k <= 0, else
+ *   when u < thr[rung][deg - 2k - 1] (drift_pt_thresholds with max_field = max degree), u the
+ *   32-bit number whose bit 31-q is bit b of plane q, plane q = word (q & 3) of
+ *   Philox((p, t, (w << 8) | (q >> 2), 10 << 24 | instance), seed);
+ *   initial word = word 0 of Philox((p, 0, w, 11 << 24 | instance), seed);
+ *   energies exact: E = 2 U - bonds, U = unsatisfied bonds.
+ * ------------------------------------------------------------------------------------------- */
+#define DRIFT_PT_GMS_MAX_DEGREE 7
+
+typedef struct DriftPtGmsProblem { /* device arrays */
+  int32_t n, n_pos, n_colors, max_degree;
+  int64_t n_bonds;
+  int32_t max_class;         /* size of the largest colour class                              */
+  int32_t reserved;
+  const int32_t* color_ptr;  /* [k+1] position ranges of the colour classes                  */
+  const int32_t* ell_nbr;    /* [max_degree][n_pos]                                           */
+  const uint8_t* degree;     /* [n_pos] (0 for padding)                                       */
+  const uint8_t* jneg;       /* [n_pos]                                                       */
+} DriftPtGmsProblem;
+
+typedef struct DriftPtGmsLayoutInfo {
+  int32_t n, n_pos, n_colors, max_degree;
+  int64_t n_bonds;
+  int32_t max_class;         /* size of the largest colour class                              */
+  int32_t reserved;
+} DriftPtGmsLayoutInfo;
+
+typedef struct DriftPtGmsLayout { /* caller-allocated host arrays sized from the info */
+  int32_t* color_ptr;        /* [k+1]                                                         */
+  int32_t* ell_nbr;          /* [max_degree][n_pos]                                           */
+  uint8_t* degree;           /* [n_pos]                                                       */
+  uint8_t* jneg;             /* [n_pos]                                                       */
+  int32_t* pos_of_site;      /* [n]                                                           */
+  int32_t* site_of_pos;      /* [n_pos] (-1 for padding)                                      */
+} DriftPtGmsLayout;
+
+typedef struct DriftPtGmsState { /* device arrays; R = 32 * n_words */
+  uint32_t* words;           /* [W][n_pos]                                                    */
+  uint32_t* best_words;      /* [W][n_pos]                                                    */
+  int64_t* energy;           /* [R]                                                           */
+  int64_t* best_energy;      /* [R]                                                           */
+  int32_t* rung_of_slot;     /* [R]                                                           */
+  int32_t* slot_of_rung;     /* [R]                                                           */
+  int64_t* swap_tried;       /* [R-1]                                                         */
+  int64_t* swap_accepted;    /* [R-1]                                                         */
+} DriftPtGmsState;
+
+typedef struct DriftPtGmsRunArgs {
+  int32_t n_words;           /* W: replicas R = 32 W                                          */
+  int32_t n_rounds, sweeps_per_round;
+  int32_t threads_per_cta;   /* 0 = automatic                                                 */
+  int64_t round_offset;
+  uint64_t seed;
+  uint32_t instance;
+  int32_t cluster_size;      /* CTAs per word: 1 = one CTA holds the word; 2..16 = a cluster   */
+                             /* splits it (shared-memory neighbour reads); 0 = automatic       */
+  const double* betas;       /* [R] device                                                    */
+  const uint32_t* thresholds;/* [R][max_degree] device, drift_pt_thresholds                   */
+  double timeout_s;
+} DriftPtGmsRunArgs;
+
+/* Host: check that every coupling is +-1 and h = 0, and size the layout (colour order of `csr`). */
+DRIFT_PT_API int drift_pt_gms_layout_query(const DriftPtCsr* csr, DriftPtGmsLayoutInfo* info);
+DRIFT_PT_API int drift_pt_gms_layout_fill(const DriftPtCsr* csr, DriftPtGmsLayout* out);
+DRIFT_PT_API int drift_pt_gms_workspace_bytes(int32_t n_words, size_t* bytes);
+/* Random initial words, exact energies, best = initial, identity rungs, zero counts. */
+DRIFT_PT_API int drift_pt_gms_init(const DriftPtGmsProblem* problem, const DriftPtGmsRunArgs* args,
+                                   DriftPtGmsState* state, void* stream);
+/* n_rounds rounds in one persistent launch; the state lives in shared memory for the whole launch.
+ * cluster_size 1: one CTA per word; 2..16: the word's positions split over a cluster (neighbour words
+ * read from the owning CTA's shared memory; same bits as cluster_size 1); 0: 1 from 16 words up, else
+ * the largest cluster the GPU holds resident for all words. Shapes that cannot be co-resident are
+ * refused with DRIFT_PT_EUNSUPPORTED. Bit-identical to any other cluster_size and to a split of the
+ * rounds over several calls (round_offset). */
+DRIFT_PT_API int drift_pt_gms_run(const DriftPtGmsProblem* problem, const DriftPtGmsRunArgs* args,
+                                  DriftPtGmsState* state, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------------------------------------------
  * Dense layer: fully connected couplings (Sherrington-Kirkpatrick type), n <= 512, R <= 512.
  * The reference runs such models through the same CSR kernel as sparse ones
  * (cuda/ising_pt.cu:109-122): every spin is its own colour class and each attempt walks n - 1

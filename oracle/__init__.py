@@ -15,7 +15,8 @@ product (``drift_b200``) imports this package.
       - ``exact``           drift/solvers/exact.py:20-49 as a Gray-code walk (n <= 30), plus
                             Boltzmann averages;
       - ``ms_run``          the bit-packed lattice chain (ms_oracle.c);
-      - ``sk_run``          the dense-coupling chain on fixed-point couplings (sk_oracle.c).
+      - ``sk_run``          the dense-coupling chain on fixed-point couplings (sk_oracle.c);
+      - ``gms_run``         the bit-packed chain on a +-1 graph (gms_oracle.c).
   * ``ref_pt`` - NumPy restatement of the reference CPU parallel tempering
     (drift/solvers/parallel_tempering.py:29-124) with the same NumPy random stream, pinned to the
     reference by golden outputs in tests/golden/.
@@ -42,7 +43,8 @@ _lib = None
 
 
 def build(force: bool = False) -> str:
-    srcs = [os.path.join(HERE, f) for f in ("pt_oracle.c", "exact.c", "ms_oracle.c", "sk_oracle.c", "Makefile")]
+    srcs = [os.path.join(HERE, f) for f in ("pt_oracle.c", "exact.c", "ms_oracle.c", "sk_oracle.c", "gms_oracle.c",
+                                             "Makefile")]
     if force or not os.path.exists(LIB_PATH) or any(os.path.getmtime(s) > os.path.getmtime(LIB_PATH) for s in srcs):
         r = subprocess.run(["make", "-s", "-C", HERE, "-B" if force else "all"], capture_output=True, text=True)
         if r.returncode != 0:
@@ -109,6 +111,17 @@ class _SkOracle(C.Structure):
                 ("accepted", C.c_void_p), ("best_history", C.c_void_p)]
 
 
+class _GmsOracle(C.Structure):
+    _fields_ = [("n", C.c_int32), ("n_pos", C.c_int32), ("k", C.c_int32), ("D", C.c_int32), ("W", C.c_int32),
+                ("n_rounds", C.c_int32), ("spr", C.c_int32), ("init", C.c_int32), ("color_ptr", C.c_void_p),
+                ("ell", C.c_void_p), ("degree", C.c_void_p), ("jneg", C.c_void_p), ("n_bonds", C.c_int64),
+                ("betas", C.c_void_p), ("thr", C.c_void_p), ("seed", C.c_uint64), ("instance", C.c_uint32),
+                ("reserved", C.c_int32), ("round_offset", C.c_int64), ("words", C.c_void_p),
+                ("best_words", C.c_void_p), ("energy", C.c_void_p), ("best_energy", C.c_void_p),
+                ("rung_of_slot", C.c_void_p), ("slot_of_rung", C.c_void_p), ("tried", C.c_void_p),
+                ("accepted", C.c_void_p)]
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -131,6 +144,8 @@ def lib():
         L.oracle_energy_fp64.restype = C.c_double
         L.oracle_ms_run.argtypes = [C.POINTER(_MsOracle)]
         L.oracle_ms_run.restype = C.c_int
+        L.oracle_gms_run.argtypes = [C.POINTER(_GmsOracle)]
+        L.oracle_gms_run.restype = C.c_int
         L.oracle_sk_run.argtypes = [C.POINTER(_SkOracle)]
         L.oracle_sk_run.restype = C.c_int
         L.oracle_sk_energy.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]
@@ -369,4 +384,44 @@ def sk_run(Jq: np.ndarray, hq: np.ndarray, shift: int, betas, scales, *, n_round
     if lib().oracle_sk_run(C.byref(o)) != 0:
         raise ValueError("oracle_sk_run failed")
     state.best_history = hist[:n_rounds]
+    return state
+
+
+class GmsState:
+    def __init__(self, W: int, n_pos: int):
+        R = 32 * W
+        self.words = np.zeros((W, n_pos), np.uint32)
+        self.best_words = np.zeros((W, n_pos), np.uint32)
+        self.energy = np.zeros(R, np.int64)
+        self.best_energy = np.zeros(R, np.int64)
+        self.rung_of_slot = np.arange(R, dtype=np.int32)
+        self.slot_of_rung = np.arange(R, dtype=np.int32)
+        self.tried = np.zeros(R, np.int64)
+        self.accepted = np.zeros(R, np.int64)
+
+
+def gms_run(layout, betas, *, n_rounds: int, sweeps_per_round: int, seed: int, instance: int = 0,
+            state: GmsState | None = None, round_offset: int = 0) -> GmsState:
+    """The bit-packed graph chain (gms_oracle.c); `layout` has n, n_pos, n_colors, max_degree,
+    n_bonds, color_ptr, ell_nbr [D][n_pos], degree, jneg (host arrays)."""
+    betas = np.ascontiguousarray(betas, np.float64)
+    R = len(betas)
+    if R % 32:
+        raise ValueError("the multispin chain needs a multiple of 32 replicas")
+    W = R // 32
+    thr = np.ascontiguousarray(thresholds(betas, layout.max_degree), np.uint32)
+    init = state is None
+    if state is None:
+        state = GmsState(W, layout.n_pos)
+    cp = np.ascontiguousarray(layout.color_ptr, np.int32)
+    ell = np.ascontiguousarray(layout.ell_nbr, np.int32)
+    deg = np.ascontiguousarray(layout.degree, np.uint8)
+    jn = np.ascontiguousarray(layout.jneg, np.uint8)
+    o = _GmsOracle(layout.n, layout.n_pos, layout.n_colors, layout.max_degree, W, n_rounds, sweeps_per_round,
+                   1 if init else 0, _p(cp), _p(ell), _p(deg), _p(jn), layout.n_bonds, _p(betas), _p(thr),
+                   seed & 0xFFFFFFFFFFFFFFFF, instance, 0, round_offset, _p(state.words), _p(state.best_words),
+                   _p(state.energy), _p(state.best_energy), _p(state.rung_of_slot), _p(state.slot_of_rung),
+                   _p(state.tried), _p(state.accepted))
+    if lib().oracle_gms_run(C.byref(o)) != 0:
+        raise ValueError("oracle_gms_run failed")
     return state

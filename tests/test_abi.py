@@ -162,6 +162,7 @@ def test_ctypes_structs_match_the_header(tmp_path):
     import subprocess
 
     from drift_b200.batch import DESC_DTYPE
+    from drift_b200.gms import GmsLayoutC, GmsLayoutInfoC, GmsProblemC, GmsRunArgsC, GmsStateC
     from drift_b200.multispin import LatticeC, MsRunArgsC, MsStateC
     from drift_b200.sk import SkProblemC, SkRunArgsC, SkStateC
 
@@ -174,7 +175,9 @@ def test_ctypes_structs_match_the_header(tmp_path):
                "DriftPtSolveResult": _lib.SolveResult, "DriftPtBatchProblem": _lib.BatchProblem,
                "DriftPtBatchRunArgs": _lib.BatchRunArgs, "DriftPtLattice": LatticeC, "DriftPtMsState": MsStateC,
                "DriftPtMsRunArgs": MsRunArgsC, "DriftPtSkProblem": SkProblemC, "DriftPtSkState": SkStateC,
-               "DriftPtSkRunArgs": SkRunArgsC}
+               "DriftPtSkRunArgs": SkRunArgsC, "DriftPtGmsProblem": GmsProblemC,
+               "DriftPtGmsLayoutInfo": GmsLayoutInfoC, "DriftPtGmsLayout": GmsLayoutC, "DriftPtGmsState": GmsStateC,
+               "DriftPtGmsRunArgs": GmsRunArgsC}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "drift_pt.h"', "int main(void) {"]
     for cname, py in mirrors.items():
         lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
