@@ -19,6 +19,7 @@
 // value the Metropolis-Hastings ratio divides by.
 #include <cstring>
 #include <cuda_bf16.h>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "../../include/drift_pt.h"
@@ -140,7 +141,7 @@ struct MadeArgs {
 // only what crosses threads in a step: the finished units' ReLU values, the next logit and the
 // drawn spins.
 template <int S, int kH1, int kH2, int kN>
-__global__ void __launch_bounds__(256) made_sample_kernel(const MadeArgs a) {
+__device__ __forceinline__ void made_sample_body(const MadeArgs& a) {
   __shared__ float r1[4][S], r2[4][S], lnext[S];
   __shared__ float xs[S];
   extern __shared__ int m_idx[];  // the degree orders: off1 [n+1], off2 [n+1], ord1 [H1], ord2 [H2]
@@ -308,6 +309,22 @@ __global__ void __launch_bounds__(256) made_sample_kernel(const MadeArgs a) {
   if (tid < ns) a.logq[base + tid] = lq;
 }
 
+template <int S, int kH1, int kH2, int kN>
+__global__ void __launch_bounds__(256) made_sample_kernel(const MadeArgs a) {
+  made_sample_body<S, kH1, kH2, kN>(a);
+}
+
+// several networks in one launch: blocks (., g) run network g with its own arguments
+template <int S, int kH1, int kH2, int kN>
+__global__ void __launch_bounds__(256) made_sample_group_kernel(const MadeArgs* args, uint32_t stream_add) {
+  MadeArgs a = args[blockIdx.y];
+  a.stream += stream_add;
+  if ((int)blockIdx.x * S >= a.count) return;
+  made_sample_body<S, kH1, kH2, kN>(a);
+}
+
+constexpr int kSampleS = 8, kSampleT = 256;
+
 // ------------------------------------------------------------------------------------------------
 // exact Metropolis-Hastings for whole-configuration proposals (dense layer state)
 // ------------------------------------------------------------------------------------------------
@@ -441,7 +458,7 @@ extern "C" int drift_pt_made_sample(const DriftPtMadeNet* net, int32_t count, in
   a.k0 = (uint32_t)(seed & 0xffffffffu);
   a.k1 = (uint32_t)(seed >> 32);
   a.stream = stream_id;
-  constexpr int S = 8, T = 256;
+  constexpr int S = kSampleS, T = kSampleT;
   a.S = S;
   // per-thread weight slices: up to 4 first-layer, 4 second-layer and 2 logit entries per unit
   if (a.h1 > 4 * T || a.h2 > 4 * T || a.n > 2 * T)
@@ -471,4 +488,73 @@ extern "C" int drift_pt_made_mh(const DriftPtSkProblem* problem, const DriftPtSk
       reinterpret_cast<long long*>(state->energy), state->best_spins, reinterpret_cast<long long*>(state->best_energy),
       state->rung_of_slot, reinterpret_cast<long long*>(prop_tried), reinterpret_cast<long long*>(prop_accepted), active);
   return made_fail("made_mh_kernel");
+}
+
+extern "C" int drift_pt_made_group_bytes(int32_t n_nets, size_t* bytes) {
+  clear_error();
+  if (n_nets < 1 || !bytes) return set_error(DRIFT_PT_EINVAL, "made_group_bytes: bad arguments");
+  *bytes = sizeof(MadeArgs) * (size_t)n_nets;
+  return DRIFT_PT_OK;
+}
+
+extern "C" int drift_pt_made_group_fill(int32_t n_nets, const DriftPtMadeNet* nets, const int32_t* counts, int32_t mode,
+                                        int8_t* const* x, float* const* logq, uint64_t seed,
+                                        const uint32_t* stream_id, void* table) {
+  clear_error();
+  if (n_nets < 1 || !nets || !counts || !x || !logq || !table || (mode != 0 && mode != 1) || (mode == 0 && !stream_id))
+    return set_error(DRIFT_PT_EINVAL, "made_group_fill: bad arguments");
+  std::vector<MadeArgs> v((size_t)n_nets);
+  for (int g = 0; g < n_nets; ++g) {
+    const DriftPtMadeNet* net = nets + g;
+    if (!net->w1t || !net->w2t || !net->w3t || !net->b1 || !net->b2 || !net->b3 || !net->ord1 || !net->off1 ||
+        !net->ord2 || !net->off2 || !x[g] || !logq[g])
+      return set_error(DRIFT_PT_EINVAL, "made_group_fill: network %d: null array", g);
+    if (net->n < 2 || net->h1 < 1 || net->h2 < 1 || counts[g] < 1 || net->max_units_per_degree > 4 ||
+        net->h1 > 4 * kSampleT || net->h2 > 4 * kSampleT || net->n > 2 * kSampleT)
+      return set_error(DRIFT_PT_EUNSUPPORTED, "made_group_fill: network %d: sizes (n <= %d, hidden <= %d)", g,
+                       2 * kSampleT, 4 * kSampleT);
+    MadeArgs& a = v[(size_t)g];
+    std::memset(&a, 0, sizeof a);
+    a.n = net->n;
+    a.h1 = net->h1;
+    a.h2 = net->h2;
+    a.S = kSampleS;
+    a.count = counts[g];
+    a.mode = mode;
+    a.w1t = static_cast<const __nv_bfloat16*>(net->w1t);
+    a.w2t = static_cast<const __nv_bfloat16*>(net->w2t);
+    a.w3t = static_cast<const __nv_bfloat16*>(net->w3t);
+    a.b1 = net->b1;
+    a.b2 = net->b2;
+    a.b3 = net->b3;
+    a.ord1 = net->ord1;
+    a.off1 = net->off1;
+    a.ord2 = net->ord2;
+    a.off2 = net->off2;
+    a.x = x[g];
+    a.logq = logq[g];
+    a.k0 = (uint32_t)(seed & 0xffffffffu);
+    a.k1 = (uint32_t)(seed >> 32);
+    a.stream = mode == 0 ? stream_id[g] : 0u;
+  }
+  const cudaError_t e = cudaMemcpy(table, v.data(), sizeof(MadeArgs) * v.size(), cudaMemcpyHostToDevice);
+  return e == cudaSuccess ? DRIFT_PT_OK : set_error(DRIFT_PT_ECUDA, "made_group_fill: upload: %s", cudaGetErrorString(e));
+}
+
+extern "C" int drift_pt_made_group_run(const void* table, int32_t n_nets, int32_t max_count, int32_t max_n,
+                                       int32_t max_h1, int32_t max_h2, uint32_t stream_add, void* stream) {
+  clear_error();
+  if (!table || n_nets < 1 || n_nets > 65535 || max_count < 1 || max_n < 2 || max_h1 < 1 || max_h2 < 1)
+    return set_error(DRIFT_PT_EINVAL, "made_group_run: bad arguments");
+  if (max_h1 > 4 * kSampleT || max_h2 > 4 * kSampleT || max_n > 2 * kSampleT)
+    return set_error(DRIFT_PT_EUNSUPPORTED, "made_group_run: hidden widths up to %d and n up to %d", 4 * kSampleT,
+                     2 * kSampleT);
+  auto fn = made_sample_group_kernel<kSampleS, 4, 4, 2>;
+  const size_t smem = (size_t)(2 * (max_n + 1) + max_h1 + max_h2) * sizeof(int);
+  int per_sm = 0;
+  const int rc = prepare_kernel((const void*)fn, kSampleT, smem, &per_sm);
+  if (rc) return rc;
+  dim3 grid((unsigned)((max_count + kSampleS - 1) / kSampleS), (unsigned)n_nets);
+  fn<<<grid, kSampleT, smem, static_cast<cudaStream_t>(stream)>>>(static_cast<const MadeArgs*>(table), stream_add);
+  return made_fail("made_sample_group_kernel");
 }

@@ -71,6 +71,26 @@ def ea_2d(L: int, seed: int) -> SparseIsingModel:
     return SparseIsingModel(L * L, i, j, w)
 
 
+def ea_2d_padded(L: int, seed: int, multiple: int = 8) -> SparseIsingModel:
+    """ea_2d(L, seed) with uncoupled spins appended up to a multiple of `multiple` spins. The extra
+    spins leave every energy unchanged; a network over all the spins then has a size the proposal
+    kernels take (a multiple of 8), and its proposals stay exact."""
+    base = ea_2d(L, seed)
+    n = -(-base.n // multiple) * multiple
+    row_ptr, col, w = base.csr()
+    rows = np.repeat(np.arange(base.n), np.diff(row_ptr))
+    keep = rows < col
+    return SparseIsingModel(n, rows[keep], col[keep], w[keep].astype(np.float64))
+
+
+def ea2d_batch(n_instances: int, seed: int, L_min: int = 8, L_max: int = 48) -> list:
+    """Uneven 2-D EA +-J instances: L_k uniform in [L_min, L_max] from `seed`, couplings of instance
+    k from seed k, each padded to a multiple of 8 spins (ea_2d_padded)."""
+    rng = np.random.default_rng(seed)
+    Ls = rng.integers(L_min, L_max + 1, size=n_instances)
+    return [ea_2d_padded(int(L), k) for k, L in enumerate(Ls)]
+
+
 def ea_3d(L: int, seed: int) -> SparseIsingModel:
     """3-D Edwards-Anderson +-J spin glass on an L^3 periodic lattice."""
     rng = np.random.default_rng(seed)

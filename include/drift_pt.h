@@ -567,6 +567,47 @@ DRIFT_PT_API int drift_pt_made_mh(const DriftPtSkProblem* problem, const DriftPt
                                   const float* logq_cur, const uint8_t* active, int64_t* prop_tried,
                                   int64_t* prop_accepted, int64_t round, void* stream);
 
+/* Several proposal networks in one launch (a batch of instances with one network each). The group
+ * table (drift_pt_made_group_bytes(n_nets) bytes of device memory, opaque) is filled once, synchronously,
+ * from the networks, their sample counts, their output buffers x[g] ([counts[g]][n_g] int8, site
+ * order) and logq[g] ([counts[g]] fp32), and a mode (0: draw, 1: evaluate the given x). Each
+ * drift_pt_made_group_run then runs network g exactly as drift_pt_made_sample would with
+ * stream_id[g] + stream_add, on blocks (., g) of one launch; max_* bound every network's sizes. */
+DRIFT_PT_API int drift_pt_made_group_bytes(int32_t n_nets, size_t* bytes);
+DRIFT_PT_API int drift_pt_made_group_fill(int32_t n_nets, const DriftPtMadeNet* nets, const int32_t* counts,
+                                          int32_t mode, int8_t* const* x, float* const* logq, uint64_t seed,
+                                          const uint32_t* stream_id, void* table);
+DRIFT_PT_API int drift_pt_made_group_run(const void* table, int32_t n_nets, int32_t max_count, int32_t max_n,
+                                         int32_t max_h1, int32_t max_h2, uint32_t stream_add, void* stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Whole-configuration proposals on a batch (integer path). Request j names rung rung[j] of
+ * instance instance[j]; requests of one call name distinct (instance, rung) pairs. Site i of
+ * instance k is position pos_of_site[site_off[k] + i] of its layout (the DriftPtLayout
+ * pos_of_site arrays of the batch's instances, concatenated).
+ * ------------------------------------------------------------------------------------------- */
+/* Copy the configuration at each requested rung, in site order, to out + out_off[j] +
+ * rep * out_step[j] (out_step may be NULL). */
+DRIFT_PT_API int drift_pt_batch_gather(const DriftPtBatchProblem* prob, const DriftPtDeviceState* state, int32_t count,
+                                       const int32_t* instance, const int32_t* rung, const int64_t* site_off,
+                                       const int32_t* pos_of_site, const int64_t* out_off, const int64_t* out_step,
+                                       int64_t rep, int8_t* out, int32_t* error_flag, void* stream);
+/* Exact Metropolis-Hastings step for independent proposals x'_j (site order, at proposals +
+ * prop_off[j]): the energy E' is recomputed exactly from the instance's layout, and x'_j replaces
+ * the configuration at (instance, rung) with probability min(1, exp(-beta (E' - E)) q(x) / q(x')),
+ * the log of the ratio in double from the exact energies and the fp32 log q values, the uniform
+ * from Philox((rung, round lo, round hi, 12 << 24 | stream id of the instance); seed). An accepted
+ * proposal below the slot's best also becomes its best. prop_tried / prop_accepted [count] are
+ * incremented per request; prop_energy [count] (may be NULL) receives E'. scratch: count *
+ * max_n_pos bytes. Out-of-range requests set *error_flag = DRIFT_PT_EINVAL and are skipped. No
+ * counterpart in the reference (the exact MH test for learned proposals is this engine's own). */
+DRIFT_PT_API int drift_pt_batch_mh(const DriftPtBatchProblem* prob, DriftPtDeviceState* state, uint64_t seed,
+                                   int32_t count, const int32_t* instance, const int32_t* rung, const int64_t* site_off,
+                                   const int32_t* pos_of_site, const int64_t* prop_off, const int8_t* proposals,
+                                   const float* logq_prop, const float* logq_cur, int64_t round, int8_t* scratch,
+                                   int64_t* prop_energy, int64_t* prop_tried, int64_t* prop_accepted,
+                                   int32_t* error_flag, void* stream);
+
 /* ---------------------------------------------------------------------------------------------
  * Host convenience: one call from host buffers to host results (the problem.bin -> result.bin
  * contract of cuda/ising_pt.cu:159-243 and drift/gpu.py:83-114). Allocates and frees device
