@@ -1,7 +1,7 @@
 """Benchmark: spin-flip attempts per ns of the B200 parallel-tempering engine.
 
     python bench.py [--gpus N] [--steps K] [--warmup W]
-                    [--workload maxcut3reg|ea2d|batched_er|ea3d64|maxcut3reg_r2048|sk512]
+                    [--workload maxcut3reg|ea2d|batched_er|ea3d64|maxcut3reg_r2048|ea2d_batch256|sk512]
                     [--impl b200|reference|reference-gpu]
 
 Workload (default ``maxcut3reg``): plain PT on MaxCut as Ising over a random 3-regular graph,
@@ -61,6 +61,15 @@ WORKLOADS = {
     "maxcut3reg_r2048": dict(desc="MaxCut random 3-regular N=4096 (J=-1), 2048 replicas (bit-packed), beta 0.2-4.0, "
                                   "2e4 sweeps in rounds of 4",
                              n=4096, seed=2, R=2048, beta=(0.2, 4.0), sweeps=20000, spr=4, bytes_per_attempt=5 / 8),
+    # uneven batch: 256 2-D EA +-J instances, L uniform in [8, 48] (seed 6), couplings of instance k
+    # from seed k, each padded with uncoupled spins to a multiple of 8 (energies unchanged); 32
+    # replicas each, beta 0.1-3.0, rounds of 10 sweeps; 1e3 sweeps per step. With --ttt: time to
+    # the best energy of a 1e5-sweep plain run, plain vs neural proposals (one MADE per instance of
+    # at most 512 spins). Algorithmic bytes per attempt as C3 with int8 couplings: 2 + 4 (4 + 1) / 32
+    "ea2d_batch256": dict(desc="256 2D EA +-J instances L~U[8,48] (padded to 8k spins), 32 replicas each, "
+                               "beta 0.1-3.0, rounds of 10 sweeps; 1e3 sweeps per step",
+                          n_instances=256, seed=6, R=32, beta=(0.1, 3.0), sweeps=1000, spr=10,
+                          bytes_per_attempt=2.0 + 4 * 5 / 32),
     # dense SK: J_ij ~ N(0, 1)/sqrt(N) (fp32 values) on the upper triangle, mirrored, h = 0, seed 4;
     # 64 replicas, beta 0.3-3.0, rounds of 10 sweeps; 1e4 sweeps per step. Tensor-core field
     # updates: the algorithmic work of an attempt is the 2N flops of J_i . s (drift/ising.py:68)
@@ -78,11 +87,20 @@ def make_batch_models(w):
 
 
 def make_model(name):
-    from drift_b200.instances import ea_2d, maxcut_3regular, sk_model
+    from drift_b200.instances import ea_2d, ea_2d_padded, er_gaussian, maxcut_3regular, sk_model
 
     w = WORKLOADS[name]
     if name == "sk512":
         return sk_model(w["n"], w["seed"])
+    # the reference runs a batch one instance at a time: its CPU sample is the median-size instance
+    if name == "batched_er":
+        sizes = np.random.default_rng(w["seed"]).integers(64, 8193, size=w["n_instances"])
+        i = int(np.argsort(sizes, kind="stable")[len(sizes) // 2])
+        return er_gaussian(int(sizes[i]), 6, 1000 + i, field_sigma=0.1)
+    if name == "ea2d_batch256":
+        Ls = np.random.default_rng(w["seed"]).integers(8, 49, size=w["n_instances"])
+        i = int(np.argsort(Ls, kind="stable")[len(Ls) // 2])
+        return ea_2d_padded(int(Ls[i]), i)
     return maxcut_3regular(w["n"], w["seed"]) if name.startswith("maxcut3reg") else ea_2d(16, w["seed"])
 
 
@@ -231,6 +249,8 @@ def bench_reference(args):
     import multiprocessing as mp
 
     w = WORKLOADS[args.workload]
+    n_sample = make_model(args.workload).n
+    where = " of the batch's median-size instance" if "n_instances" in w else ""
     cores = os.cpu_count() or 1
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores) as pool:
@@ -248,10 +268,10 @@ def bench_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": w["desc"], "sample": f"{cores} processes x (1 round x 1 sweep x "
-                   f"{min(w['R'], REF_SAMPLE_RUNGS)} rungs x {w['n']} spins) per step"},
+                   f"{min(w['R'], REF_SAMPLE_RUNGS)} rungs x {n_sample} spins{where}) per step"},
         "cpu_baseline": {"value": v, "unit": "flips/ns", "cores": cores, "kind": "port",
                          "sample": f"oracle/ref_pt.py (reference CPU PT restated, same NumPy stream), one process per core, "
-                                   f"{cores} x {min(w['R'], REF_SAMPLE_RUNGS) * w['n']:.0f} attempts per step"},
+                                   f"{cores} x {min(w['R'], REF_SAMPLE_RUNGS) * n_sample:.0f} attempts per step"},
         "e2e": {"value": v, "unit": "flips/ns", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -956,6 +976,182 @@ def bench_batched(args):
         dist.destroy_process_group()
 
 
+def ttt_batch(w, bp, hps, args, dev):
+    """Time for every instance of the batch to reach the best energy of a 10x longer plain run:
+    plain batched PT vs the same with neural proposals (sample collection, network construction
+    and training inside the clock). Per instance the first time its best reaches its target is
+    kept; the batch's time is the last of them (None when the cap came first)."""
+    import torch
+
+    from drift_b200.batch import BatchEngine
+    from drift_b200.batch_neural import BatchNeuralPT, make_nets
+
+    spr, chunk = w["spr"], 10
+    K = bp.n_instances
+    ref = BatchEngine(bp, seed=100, sweeps_per_round=spr)
+    ref.init()
+    t_ref0 = time.perf_counter()
+    ref_rounds = args.ttt_ref_sweeps // spr
+    done = 0
+    while done < ref_rounds:
+        ref.run(min(500, ref_rounds - done))
+        done += min(500, ref_rounds - done)
+    ref.check()
+    target = ref.best_energies()
+    t_ref = time.perf_counter() - t_ref0
+    sizes = np.array([int(d["n"]) for d in bp.desc])
+
+    def track(step, eng, cap):
+        t0 = time.perf_counter()
+        first = np.full(K, np.nan)
+        while time.perf_counter() - t0 < cap:
+            step()
+            hit = eng.best_energies() <= target
+            now = time.perf_counter() - t0
+            first[np.isnan(first) & hit] = now
+            if not np.isnan(first).any():
+                break
+        return first
+
+    def summary(first, extra=None):
+        ok = ~np.isnan(first)
+        small = sizes <= 512
+        r = {"all_reached_s": float(first.max()) if ok.all() else None, "fraction_reached": float(ok.mean()),
+             "median_instance_s": float(np.median(first[ok])) if ok.any() else None,
+             "median_instance_s_n_le_512": float(np.median(first[ok & small])) if (ok & small).any() else None,
+             "reached_n_le_512": float(ok[small].mean())}
+        r.update(extra or {})
+        return r
+
+    out = {"target_from": f"plain batched PT, seed 100, {args.ttt_ref_sweeps} sweeps ({t_ref:.1f} s)",
+           "cap_s": args.ttt_cap_s, "networks": int((sizes <= 512).sum()), "plain": [], "neural": []}
+    for seed in range(1, args.ttt_seeds + 1):
+        eng = BatchEngine(bp, seed=seed, sweeps_per_round=spr)
+        eng.init()
+        torch.cuda.synchronize()
+        first = track(lambda: eng.run(chunk), eng, args.ttt_cap_s)
+        out["plain"].append(summary(first, {"seed": seed}))
+        eng = BatchEngine(bp, seed=seed, sweeps_per_round=spr)
+        eng.init()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        nets = make_nets(bp, seed=seed)
+        bn = BatchNeuralPT(eng, nets, n_cold=8)
+        data = bn.collect(args.ttt_batch_rounds)
+        t_collect = time.perf_counter() - t0
+        for k, m in nets.items():
+            m.train(data[k], epochs=args.ttt_epochs, batch=args.ttt_batch_size, lr=args.ttt_lr)
+        torch.cuda.synchronize()
+        t_train = time.perf_counter() - t0 - t_collect
+        every = max(1, min(chunk, args.ttt_propose_every))
+
+        def neural_step():
+            # chunk rounds, a proposal after every `every`-th
+            for r in range(chunk):
+                if (r + 1) % every == 0:
+                    bn.run(1)
+                else:
+                    eng.run(1)
+        # instances that reached their target during collection count at its end (an upper bound)
+        reached_early = eng.best_energies() <= target
+        first = track(neural_step, eng, args.ttt_cap_s - t_collect - t_train) + (t_collect + t_train)
+        first[reached_early] = t_collect
+        acc = bn.acceptance()
+        out["neural"].append(summary(first, {"seed": seed, "collect_s": t_collect, "train_s": t_train,
+                                             "propose_every_rounds": every, "epochs": args.ttt_epochs,
+                                             "lr": args.ttt_lr, "train_samples_per_net": 8 * args.ttt_batch_rounds,
+                                             "proposal_acceptance_mean": float(np.nanmean(list(acc.values()))),
+                                             "proposal_acceptance_max": float(np.nanmax(list(acc.values())))}))
+    for k in ("plain", "neural"):
+        v = [r["all_reached_s"] for r in out[k]]
+        out[k + "_all_reached_median_s"] = float(np.median(v)) if all(x is not None for x in v) else None
+    if out["plain_all_reached_median_s"] and out["neural_all_reached_median_s"]:
+        out["speedup_neural_over_plain"] = out["plain_all_reached_median_s"] / out["neural_all_reached_median_s"]
+    return out
+
+
+def bench_ea2d_batch(args):
+    import torch
+
+    from drift_b200.batch import BatchEngine, BatchProblem, autotune
+    from drift_b200.engine import HostProblem
+    from drift_b200.instances import ea2d_batch
+
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    w = WORKLOADS[args.workload]
+    models = ea2d_batch(w["n_instances"], w["seed"])
+    hps = [HostProblem.from_model(m) for m in models]
+    ladders = [ladder(w)] * len(hps)
+    bp = BatchProblem(hps, ladders, stream_ids=np.arange(len(hps)) + 1024 * rank, device=dev)
+    rounds = args.rounds or w["sweeps"] // w["spr"]
+    eng = BatchEngine(bp, seed=1, sweeps_per_round=w["spr"])
+    eng.init()
+    shape = autotune(eng, rounds=2)
+    total_n = int(sum(int(d["n"]) for d in bp.desc))
+    attempts_per_step = float(w["R"]) * total_n * rounds * w["spr"]
+    for _ in range(args.warmup):
+        eng.run(rounds)
+    eng.check()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    t_steps = 0.0
+    for s_ in range(args.steps):
+        flush.fill_(s_ & 0xFF)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        eng.run(rounds)
+        e1.record()
+        e1.synchronize()
+        t_steps += e0.elapsed_time(e1) * 1e-3
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    eng.check()
+    t_max = reduce_max(t_steps, world, dev)
+    value = attempts_per_step * args.steps * world / t_max / 1e9
+    t0 = time.perf_counter()
+    bp2 = BatchProblem(hps, ladders, stream_ids=np.arange(len(hps)) + 1024 * rank, device=dev)
+    e2 = BatchEngine(bp2, seed=2, sweeps_per_round=w["spr"], **shape)
+    e2.init()
+    e2.run(rounds)
+    best = e2.best_energies()
+    t_e2e = reduce_max(time.perf_counter() - t0, world, dev)
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        achieved = attempts_per_step * w["bytes_per_attempt"] / (t_max / args.steps) / 1e9
+        h2d = int(sum(t.numel() * t.element_size() for t in (bp2.d_desc, bp2.d_color_ptr, bp2.d_slice_off,
+                                                             bp2.d_ell_nbr, bp2.d_ell_w, bp2.d_h_pos, bp2.d_betas)))
+        line = {
+            "metric": "spin-flips/ns", "value": value, "unit": "flips/ns", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int8", "data": "synthetic",
+            "config": {"workload": w["desc"], "instances": len(hps), "total_spins": total_n, "rounds": rounds,
+                       "sweeps_per_round": w["spr"], "attempts_per_step": attempts_per_step,
+                       "parallelism": f"replicas-only x{world}", "l2": "flushed between steps (256 MiB write)",
+                       "launch": shape},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_kind": peak_kind, "kernel": "pt_batched_kernel",
+                         "bytes_per_attempt": w["bytes_per_attempt"]},
+            "e2e": {"value": attempts_per_step * world / t_e2e / 1e9, "unit": "flips/ns", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": int(bp2.total_slots * 8), "api": "BatchProblem + BatchEngine (Python)",
+                    "best_energy_mean": float(np.mean(best))},
+            "gpu_launches": args.steps,
+            "clocks": clocks,
+        }
+        if args.ttt and world == 1:
+            line["time_to_target"] = ttt_batch(w, bp, hps, args, dev)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -971,6 +1167,12 @@ def main():
     ap.add_argument("--ttt-ref-sweeps", type=int, default=100000)
     ap.add_argument("--ttt-samples", type=int, default=100000)
     ap.add_argument("--ttt-epochs", type=int, default=5)
+    ap.add_argument("--ttt-lr", type=float, default=1e-3, help="neural PT: Adam learning rate")
+    ap.add_argument("--ttt-batch-size", type=int, default=512, help="neural PT: training batch")
+    ap.add_argument("--ttt-propose-every", type=int, default=1,
+                    help="batched neural PT: rounds between proposals (1 = after every round)")
+    ap.add_argument("--ttt-batch-rounds", type=int, default=256,
+                    help="batched neural PT: plain rounds that collect each network's training set (8 per round)")
     ap.add_argument("--rounds", type=int, default=0,
                     help="override the rounds per step (profiling of a short case; the line then says so)")
     args = ap.parse_args()
@@ -986,6 +1188,8 @@ def main():
         bench_ms(args)
     elif args.workload == "maxcut3reg_r2048":
         bench_gms(args)
+    elif args.workload == "ea2d_batch256":
+        bench_ea2d_batch(args)
     else:
         bench_b200(args)
 
