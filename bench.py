@@ -206,6 +206,12 @@ def reduce_max(x: float, world: int, device) -> float:
     return float(t.item())
 
 
+def whole_job_rate(attempts_per_rank_step: float, steps: int, world: int, t_max_s: float) -> float:
+    """Whole-job spin-flips/ns: every rank's attempts (replicas only: each rank runs its own copy of
+    the job) over the slowest rank's device time."""
+    return attempts_per_rank_step * steps * world / t_max_s / 1e9
+
+
 def barrier(world: int):
     if world > 1:
         import torch.distributed as dist
@@ -403,7 +409,7 @@ def bench_b200(args):
     eng.check()
     t_max = reduce_max(t_steps, world, dev)
     tk_max = reduce_max(t_kernel, world, dev)
-    value = attempts_per_step * args.steps * world / t_max / 1e9
+    value = whole_job_rate(attempts_per_step, args.steps, world, t_max)
 
     # ---- end to end through the C ABI with host buffers ----
     L = _lib.load()
@@ -539,7 +545,7 @@ def bench_sk(args):
     best = eng.fetch()["best_energy"].min() * sk.energy_unit
     t_max = reduce_max(t_steps, world, dev)
     tk_max = reduce_max(t_kernel, world, dev)
-    value = attempts_per_step * args.steps * world / t_max / 1e9
+    value = whole_job_rate(attempts_per_step, args.steps, world, t_max)
     # end to end through the public Python API: quantisation and coupling table on the host, upload,
     # initialisation, the rounds, results downloaded
     e2e_steps = max(1, min(args.steps, 3))
@@ -657,7 +663,7 @@ def bench_ms(args):
     eng.check()
     t_max = reduce_max(t_steps, world, dev)
     tk_max = reduce_max(t_kernel, world, dev)
-    value = attempts_per_step * args.steps * world / t_max / 1e9
+    value = whole_job_rate(attempts_per_step, args.steps, world, t_max)
     # end to end through the public Python API: couplings built on the host, uploaded, init, rounds,
     # energies downloaded
     e2e_steps = max(1, min(args.steps, 3))
@@ -769,7 +775,7 @@ def bench_gms(args):
     eng.check()
     t_max = reduce_max(t_steps, world, dev)
     tk_max = reduce_max(t_kernel, world, dev)
-    value = attempts_per_step * args.steps * world / t_max / 1e9
+    value = whole_job_rate(attempts_per_step, args.steps, world, t_max)
     # end to end through the public Python API: layout built on the host from the model, uploaded,
     # init, rounds, best energies downloaded
     e2e_steps = max(1, min(args.steps, 3))
@@ -937,7 +943,7 @@ def bench_batched(args):
     clocks = sampler.stop()
     eng.check()
     t_max = reduce_max(t_steps, world, dev)
-    value = attempts_per_step * args.steps * world / t_max / 1e9
+    value = whole_job_rate(attempts_per_step, args.steps, world, t_max)
     # end to end through the public Python API: layouts and state uploaded from host, run, best
     # energies downloaded
     t0 = time.perf_counter()
@@ -1113,7 +1119,7 @@ def bench_ea2d_batch(args):
     clocks = sampler.stop()
     eng.check()
     t_max = reduce_max(t_steps, world, dev)
-    value = attempts_per_step * args.steps * world / t_max / 1e9
+    value = whole_job_rate(attempts_per_step, args.steps, world, t_max)
     t0 = time.perf_counter()
     bp2 = BatchProblem(hps, ladders, stream_ids=np.arange(len(hps)) + 1024 * rank, device=dev)
     e2 = BatchEngine(bp2, seed=2, sweeps_per_round=w["spr"], **shape)
