@@ -1,4 +1,4 @@
-"""Per-rung observables of a PT run (SURVEY a'9): energy, |magnetisation| and, from two independent
+"""Per-rung observables of a PT run: energy, |magnetisation| and, from two independent
 ladders, the overlap q = (1/n) sum_i s_i^a s_i^b, recorded after every round, plus blocked means
 and standard errors for comparing runs."""
 
