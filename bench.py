@@ -1141,7 +1141,8 @@ def bench_ea2d_batch(args):
                        "parallelism": f"replicas-only x{world}", "l2": "flushed between steps (256 MiB write)",
                        "launch": shape},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "peak_kind": peak_kind, "kernel": "pt_batched_kernel",
+                         "traffic": load_traffic("pt_batched_kernel/ea2d_batch256"), "peak_kind": peak_kind,
+                         "kernel": "pt_batched_kernel",
                          "bytes_per_attempt": w["bytes_per_attempt"]},
             "e2e": {"value": attempts_per_step * world / t_e2e / 1e9, "unit": "flips/ns", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": int(bp2.total_slots * 8), "api": "BatchProblem + BatchEngine (Python)",
