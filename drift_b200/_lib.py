@@ -27,7 +27,7 @@ EXPORTED = (
     "drift_pt_colsum_bf16", "drift_pt_adam", "drift_pt_made_sample", "drift_pt_made_mh",
     "drift_pt_gms_layout_query", "drift_pt_gms_layout_fill", "drift_pt_gms_workspace_bytes", "drift_pt_gms_init",
     "drift_pt_gms_run", "drift_pt_made_group_bytes", "drift_pt_made_group_fill", "drift_pt_made_group_run",
-    "drift_pt_batch_gather", "drift_pt_batch_mh",
+    "drift_pt_batch_gather", "drift_pt_batch_mh", "drift_pt_batch_layout_query", "drift_pt_batch_layout_fill",
 )
 
 vp = C.c_void_p

@@ -30,6 +30,27 @@ assert DESC_DTYPE.itemsize == 88
 SPIN_BUDGET = 160 * 1024  # shared-memory bytes for one item's spins
 
 
+class BatchSizesC(C.Structure):
+    _fields_ = [("color_ptr", C.c_int64), ("slice_off", C.c_int64), ("ell", C.c_int64), ("pos", C.c_int64),
+                ("sites", C.c_int64), ("all_integer", C.c_int32), ("reserved", C.c_int32)]
+
+
+class BatchLayoutC(C.Structure):
+    _fields_ = [("color_ptr", C.c_void_p), ("slice_off", C.c_void_p), ("ell_nbr", C.c_void_p), ("ell_w", C.c_void_p),
+                ("h_pos", C.c_void_p), ("site_of_pos", C.c_void_p), ("pos_of_site", C.c_void_p)]
+
+
+def _bind():
+    L = _lib.load()
+    if not getattr(L, "_blay_bound", False):
+        vp = C.c_void_p
+        L.drift_pt_batch_layout_query.argtypes = [C.c_int32, vp, vp, C.POINTER(BatchSizesC)]
+        L.drift_pt_batch_layout_fill.argtypes = [C.c_int32, vp, vp, C.c_int32, vp, vp, vp, vp, vp,
+                                                 C.POINTER(BatchLayoutC)]
+        L._blay_bound = True
+    return L
+
+
 class BatchProblem:
     """Concatenated device layouts of several HostProblems with a ladder (betas) each."""
 
@@ -39,88 +60,67 @@ class BatchProblem:
 
         if len(problems) != len(ladders) or not problems:
             raise ValueError("need one ladder per problem")
-        L = _lib.load()
-        infos = []
-        for hp in problems:
-            info = _lib.LayoutInfo()
-            _lib.check(L.drift_pt_layout_query(C.byref(hp.c_csr()), C.byref(info)), "layout_query")
-            infos.append(info)
-        all_int = all(i.integer_couplings for i in infos)
+        L = _bind()
+        K = len(problems)
+        csrs = (_lib.Csr * K)(*[hp.c_csr() for hp in problems])
+        infos = (_lib.LayoutInfo * K)()
+        sizes = BatchSizesC()
+        _lib.check(L.drift_pt_batch_layout_query(K, csrs, infos, C.byref(sizes)), "drift_pt_batch_layout_query")
+        all_int = bool(sizes.all_integer)
         if integer_path is None:
             integer_path = all_int
         if integer_path and not all_int:
             raise ValueError("integer path requested but some instance has non-integer couplings")
         self.integer_path = bool(integer_path)
-        self.n_instances = K = len(problems)
+        self.n_instances = K
         self.stream_ids = np.arange(K, dtype=np.int64) if stream_ids is None else np.asarray(stream_ids, np.int64)
         if self.stream_ids.shape != (K,) or np.any(self.stream_ids < 0) or np.any(self.stream_ids >= 2 ** 24):
             raise ValueError("stream_ids must be K values in [0, 2^24)")
         self.ladders = [np.ascontiguousarray(b, dtype=np.float64) for b in ladders]
+        R = np.array([len(b) for b in self.ladders], np.int32)
+        if np.any(R < 1):
+            raise ValueError(f"instance {int(np.argmin(R))}: empty ladder")
+        betas = np.concatenate(self.ladders)
+        F = np.array([i.max_field for i in infos], np.int64) if self.integer_path else np.zeros(K, np.int64)
+        wd = np.int8 if self.integer_path else np.float32
+        hd = np.int32 if self.integer_path else np.float32
+        cp = np.zeros(sizes.color_ptr, np.int32)
+        so = np.zeros(sizes.slice_off, np.int32)
+        nb = np.zeros(sizes.ell + 4, np.int32)  # tails: the kernels may read a vector past the last entry
+        w = np.zeros(sizes.ell + 16, wd)
+        h = np.zeros(sizes.pos, hd)
+        sop = np.zeros(sizes.pos, np.int32)
+        pos = np.zeros(sizes.sites, np.int32)
+        thr = np.zeros(max(int((R * F).sum()), 1), np.uint32)
         desc = np.zeros(K, dtype=DESC_DTYPE)
-        cps, sos, nbrs, ws, hs, betas, thrs = [], [], [], [], [], [], []
-        self.site_of_pos, self.pos_of_site = [], []
-        off = dict(cp=0, so=0, ell=0, pos=0, slot=0, spin=0, thr=0)
-        for k, (hp, info, b) in enumerate(zip(problems, infos, self.ladders)):
-            R = len(b)
-            if R < 1:
-                raise ValueError(f"instance {k}: empty ladder")
-            cp = np.zeros(info.n_colors + 1, np.int32)
-            so = np.zeros(info.n_slices + 1, np.int32)
-            nb = np.zeros(max(info.n_ell, 1), np.int32)
-            w = np.zeros(max(info.n_ell, 1), np.int8 if self.integer_path else np.float32)
-            h = np.zeros(info.n_pos, np.int32 if self.integer_path else np.float32)
-            sop = np.zeros(info.n_pos, np.int32)
-            pos = np.zeros(info.n, np.int32)
-            lay = _lib.Layout(_ptr(cp), _ptr(so), _ptr(nb), _ptr(w), _ptr(h), _ptr(sop), _ptr(pos))
-            _lib.check(L.drift_pt_layout_fill(C.byref(hp.c_csr()), 1 if self.integer_path else 0, C.byref(lay)),
-                       "layout_fill")
-            F = info.max_field if self.integer_path else 0
-            d = desc[k]
-            d["n"], d["n_pos"], d["n_slices"], d["n_colors"] = info.n, info.n_pos, info.n_slices, info.n_colors
-            d["n_replicas"], d["max_field"], d["stream_id"] = R, F, int(self.stream_ids[k])
-            d["color_ptr"], d["slice_off"], d["ell"], d["pos"] = off["cp"], off["so"], off["ell"], off["pos"]
-            d["slot0"], d["spin0"], d["thr"] = off["slot"], off["spin"], off["thr"]
-            cps.append(cp)
-            sos.append(so)
-            nbrs.append(nb[: info.n_ell])
-            ws.append(w[: info.n_ell])
-            hs.append(h)
-            betas.append(b)
-            if self.integer_path:
-                t = np.zeros(R * F, np.uint32)
-                _lib.check(L.drift_pt_thresholds(R, _ptr(b), F, _ptr(t)), "thresholds")
-                thrs.append(t)
-                off["thr"] += R * F
-            self.site_of_pos.append(sop)
-            self.pos_of_site.append(pos)
-            off["cp"] += cp.size
-            off["so"] += so.size
-            off["ell"] += info.n_ell
-            off["pos"] += info.n_pos
-            off["slot"] += R
-            off["spin"] += R * info.n_pos
+        out = BatchLayoutC(_ptr(cp), _ptr(so), _ptr(nb), _ptr(w), _ptr(h), _ptr(sop), _ptr(pos))
+        sid = self.stream_ids.astype(np.int32)
+        _lib.check(L.drift_pt_batch_layout_fill(K, csrs, infos, 1 if self.integer_path else 0, _ptr(R), _ptr(sid),
+                                                _ptr(betas), desc.ctypes.data, _ptr(thr), C.byref(out)),
+                   "drift_pt_batch_layout_fill")
         self.desc = desc
-        self.infos = infos
-        self.total_slots = off["slot"]
-        self.total_spin_bytes = off["spin"]
+        self.infos = list(infos)
+        self.site_of_pos = [sop[int(d["pos"]): int(d["pos"]) + int(d["n_pos"])] for d in desc]
+        site0 = np.concatenate([[0], np.cumsum([int(d["n"]) for d in desc])])
+        self.pos_of_site = [pos[site0[k]: site0[k + 1]] for k in range(K)]
+        self.total_slots = int(R.sum())
+        self.total_spin_bytes = int(sum(int(d["n_replicas"]) * int(d["n_pos"]) for d in desc))
         self.max_n_pos = int(max(i.n_pos for i in infos))
         self.max_colors = int(max(i.n_colors for i in infos))
         self.max_width = int(max(i.max_degree for i in infos))
         self.min_width = int(min(i.min_width for i in infos))
-        self.max_field = int(max(i.max_field for i in infos)) if self.integer_path else 0
+        self.max_field = int(F.max()) if self.integer_path else 0
         self.has_field = int(any(i.has_field for i in infos))
         self.device = dev = torch.device(device)
-        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
-        cat = lambda xs, dt: np.concatenate(xs).astype(dt) if xs else np.zeros(1, dt)
+        t = lambda a: torch.from_numpy(a).to(dev)
         self.d_desc = t(desc.view(np.uint8))
-        self.d_color_ptr = t(cat(cps, np.int32))
-        self.d_slice_off = t(cat(sos, np.int32))
-        self.d_ell_nbr = t(np.concatenate([cat(nbrs, np.int32), np.zeros(4, np.int32)]))
-        wd = np.int8 if self.integer_path else np.float32
-        self.d_ell_w = t(np.concatenate([cat(ws, wd), np.zeros(16, wd)]))
-        self.d_h_pos = t(cat(hs, np.int32 if self.integer_path else np.float32))
-        self.d_betas = t(cat(betas, np.float64))
-        self.d_thr = t(cat(thrs, np.uint32).view(np.int32)) if self.integer_path else None
+        self.d_color_ptr = t(cp)
+        self.d_slice_off = t(so)
+        self.d_ell_nbr = t(nb)
+        self.d_ell_w = t(w)
+        self.d_h_pos = t(h)
+        self.d_betas = t(betas)
+        self.d_thr = t(thr.view(np.int32)) if self.integer_path else None
 
     def c_problem(self) -> "_lib.BatchProblem":
         return _lib.BatchProblem(self.n_instances, 1 if self.integer_path else 0, self.has_field, self.max_width,

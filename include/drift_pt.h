@@ -253,6 +253,35 @@ typedef struct DriftPtBatchProblem {
   const uint32_t* thresholds;/* integer path: [R_k][F_k] per instance at desc.thr           */
 } DriftPtBatchProblem;
 
+/* Layout of a whole batch in two calls (the per-instance layout query/fill of every instance, with
+ * the descriptor offsets and the threshold tables): drift_pt_batch_layout_query sizes the
+ * concatenated arrays and returns each instance's DriftPtLayoutInfo; drift_pt_batch_layout_fill
+ * writes instance k's layout at its offsets (desc[k]) and, on the integer path, its thresholds
+ * [R_k][F_k] from betas (concatenated, R_k per instance). Instances are split over the host's
+ * threads. Replaces the per-instance host loop of a batch (drift/gpu.py:69-81 once per instance). */
+typedef struct DriftPtBatchSizes {
+  int64_t color_ptr, slice_off, ell, pos, sites; /* element counts of the concatenated arrays    */
+  int32_t all_integer;       /* 1 if every instance has integer couplings                    */
+  int32_t reserved;
+} DriftPtBatchSizes;
+
+typedef struct DriftPtBatchLayout { /* caller-allocated, sized from DriftPtBatchSizes */
+  int32_t* color_ptr;        /* [color_ptr]                                                  */
+  int32_t* slice_off;        /* [slice_off]                                                  */
+  int32_t* ell_nbr;          /* [ell]                                                        */
+  void* ell_w;               /* [ell] int8 (integer path) or float                           */
+  void* h_pos;               /* [pos] int32 (integer path) or float                          */
+  int32_t* site_of_pos;      /* [pos]                                                        */
+  int32_t* pos_of_site;      /* [sites]: instance k's at the sum of the earlier instances' n  */
+} DriftPtBatchLayout;
+
+DRIFT_PT_API int drift_pt_batch_layout_query(int32_t n_instances, const DriftPtCsr* csrs, DriftPtLayoutInfo* infos,
+                                             DriftPtBatchSizes* sizes);
+DRIFT_PT_API int drift_pt_batch_layout_fill(int32_t n_instances, const DriftPtCsr* csrs, const DriftPtLayoutInfo* infos,
+                                            int32_t integer_path, const int32_t* n_replicas, const int32_t* stream_ids,
+                                            const double* betas, DriftPtInstanceDesc* desc, uint32_t* thresholds,
+                                            DriftPtBatchLayout* out);
+
 /* Work items: one item = replicas [first, first + count) of one instance, processed by one CTA
  * for a round. items[3*i] = instance, items[3*i+1] = first local slot, items[3*i+2] = count.
  * Order them largest first for load balance (drift_pt_batch_items does). */
