@@ -20,7 +20,8 @@ from conftest import cuda_ready, dense_from_edges
 from drift_b200 import _lib
 from drift_b200.engine import DeviceProblem, HostProblem, PtEngine, geometric_betas
 from drift_b200.gpu import parallel_tempering_gpu
-from drift_b200.instances import ea_2d, er_gaussian, maxcut_3regular, pm_spin_glass, random_graph, maxcut_ising, sk_model
+from drift_b200.instances import (ea_2d, er_gaussian, gnp_pm, maxcut_3regular, maxcut_ising, pm_spin_glass,
+                                  random_graph, sk_model)
 
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not cuda_ready(), reason="needs CUDA and libdrift_pt.so")]
 
@@ -72,6 +73,47 @@ CASES = {
     "er_gaussian_2000_fp32": (lambda: er_gaussian(2000, 6, 3), 8, (1 / 3.0, 10.0), 12, 2, 3),
     "sk_64_dense_fp32": (lambda: sk_model(64, 4), 8, (1 / 3.0, 1 / 0.3), 40, 2, 4),
 }
+
+
+def _isolated_spins():
+    from drift_b200.ising import IsingModel
+
+    J = gnp_pm(30, 0.15, 1).J.copy()
+    J[:5] = 0.0
+    J[:, :5] = 0.0
+    return IsingModel(J, np.zeros(30))
+
+
+def _pure_field(n, values, seed):
+    from drift_b200.ising import IsingModel
+
+    rng = np.random.default_rng(seed)
+    h = rng.normal(size=n) if values is None else rng.choice(values, size=n)
+    return IsingModel(np.zeros((n, n)), h)
+
+
+EDGE_CASES = {
+    # one replica (no exchange pair), two, an odd count; ragged sizes (25, 257 spins); isolated spins;
+    # no couplings at all (an empty coupling table) on the fp32 and the integer path
+    "one_replica": (lambda: maxcut_ising(random_graph(16, 0.5, 3)), 1, (0.2, 5.0), 60, 2, 5),
+    "two_replicas": (lambda: maxcut_ising(random_graph(16, 0.5, 3)), 2, (0.2, 5.0), 60, 2, 6),
+    "odd_ladder_ragged_25": (lambda: ea_2d(5, 2), 7, (0.2, 5.0), 80, 3, 7),
+    "isolated_spins": (_isolated_spins, 9, (0.2, 5.0), 60, 2, 8),
+    "ragged_257": (lambda: gnp_pm(257, 0.02, 4), 10, (0.2, 5.0), 40, 2, 9),
+    "no_couplings_fp32": (lambda: _pure_field(12, None, 3), 6, (0.2, 5.0), 50, 2, 10),
+    "no_couplings_int": (lambda: _pure_field(11, [-2.0, -1.0, 1.0, 2.0], 4), 5, (0.2, 5.0), 50, 2, 11),
+}
+
+
+@pytest.mark.parametrize("name", list(EDGE_CASES))
+def test_edge_cases_match_oracle_bit_exact(name):
+    make, R, (tmin, tmax), rounds, spr, seed = EDGE_CASES[name]
+    model = make()
+    betas = geometric_betas(R, tmin, tmax)
+    hp, prob, eng, st, hist = run_engine(model, betas, rounds, spr, seed)
+    ost = oracle.pt_run(oracle_problem(hp, prob.integer_path), betas, n_rounds=rounds, sweeps_per_round=spr,
+                        seed=seed, thr=eng.thr)
+    assert_bit_exact(st, ost, hist, rounds)
 
 
 @pytest.mark.parametrize("name", list(CASES))
