@@ -273,6 +273,8 @@ extern "C" int drift_pt_run(const DriftPtDeviceProblem* prob, const DriftPtRunAr
   a.err = reinterpret_cast<int*>(ws + 8);
   a.pub = reinterpret_cast<long long*>(ws + kWsHeader);
   a.tags = reinterpret_cast<unsigned long long*>(ws + kWsHeader + half);
+  // integer energies obey |E| <= n F: below 2^31 they travel with their round tag in one word
+  a.packed = prob->integer_path && (long long)prob->n * prob->max_field < (1ll << 31) ? 1 : 0;
   const double to = args->timeout_s > 0 ? args->timeout_s : 10.0;
   a.timeout_ns = (long long)(to * 1e9);
   cudaStream_t st = static_cast<cudaStream_t>(stream);

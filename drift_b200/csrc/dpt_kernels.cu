@@ -39,6 +39,16 @@ __device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned l
   asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
 __device__ __forceinline__ int ld_relaxed_i32(const int* p) {
   int v;
   asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -199,10 +209,16 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelAr
       imp[i] = (e < ebest[i]) ? 1 : 0;
       if (e < ebest[i]) ebest[i] = e;
       if (gridDim.x > 1) {
-        // publish: the energy, then (release-ordered after it) the round tag that readers poll
         const size_t at = (size_t)(round & 1) * R + s0 + i;
-        __stcg(a.pub + at, e);
-        st_release_u64(a.tags + at, (unsigned long long)round + 1ull);
+        if (a.packed) {
+          // energy and round tag in one single-copy-atomic word: no ordering between two words needed
+          st_relaxed_u64(reinterpret_cast<unsigned long long*>(a.pub) + at,
+                         ((unsigned long long)(uint32_t)(round + 1) << 32) | (uint32_t)(int32_t)e);
+        } else {
+          // publish: the energy, then (release-ordered after it) the round tag that readers poll
+          __stcg(a.pub + at, e);
+          st_release_u64(a.tags + at, (unsigned long long)round + 1ull);
+        }
       }
     }
     __syncthreads();
@@ -221,6 +237,24 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelAr
       const unsigned long long want = (unsigned long long)round + 1ull;
       for (int s = tid; s < R && !abort_now; s += B) {
         const size_t at = (size_t)(round & 1) * R + s;
+        if (a.packed) {
+          const unsigned long long* pw = reinterpret_cast<const unsigned long long*>(a.pub) + at;
+          const uint32_t tag = (uint32_t)want;
+          unsigned long long v = ld_relaxed_u64(pw);
+          if ((uint32_t)(v >> 32) != tag) {
+            const unsigned long long t0 = global_timer_ns();
+            while ((uint32_t)((v = ld_relaxed_u64(pw)) >> 32) != tag) {
+              if (ld_relaxed_i32(a.err) != 0) { abort_now = 1; break; }
+              if (global_timer_ns() - t0 > (unsigned long long)a.timeout_ns) {
+                atomicExch(a.err, DRIFT_PT_ETIMEOUT);
+                abort_now = 1;
+                break;
+              }
+            }
+          }
+          if (!abort_now) eall[s] = (long long)(int32_t)(uint32_t)v;
+          continue;
+        }
         if (ld_acquire_u64(a.tags + at) < want) {
           const unsigned long long t0 = global_timer_ns();
           while (ld_acquire_u64(a.tags + at) < want) {

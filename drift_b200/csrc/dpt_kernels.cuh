@@ -35,6 +35,7 @@ struct PtKernelArgs {
   int* err;
   long long* pub;                // [2][R] energies published per round parity
   unsigned long long* tags;      // [2][R] round + 1 once the matching energy is visible
+  int packed;                    // 1: pub holds (round + 1) << 32 | int32 energy words, tags unused
   long long timeout_ns;
 };
 
