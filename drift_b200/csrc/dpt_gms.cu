@@ -12,8 +12,10 @@
 // In a round's last sweep each position also counts, after its update, the unsatisfied bonds to
 // neighbours of lower colour (positions before its class): every bond is counted once, at its
 // higher-colour end, with both ends final for the round. The per-replica totals give the exact
-// energies E = 2U - bonds. The W CTAs then publish their energies with round tags, each gathers all
-// R, and every CTA evaluates the same adjacent-rung exchange (all waits bounded by a time limit).
+// energies E = 2U - bonds (|E| < 2^31). The W CTAs then publish each energy with its round tag as
+// one 64-bit word (a relaxed single-copy-atomic store, no fence), every CTA gathers all R with all
+// its threads, and every CTA evaluates the same adjacent-rung exchange (all waits bounded by a time
+// limit).
 #include <climits>
 #include <cstring>
 #include <cuda_runtime.h>
@@ -82,13 +84,14 @@ __device__ __forceinline__ unsigned long long gms_now() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-__device__ __forceinline__ unsigned long long gms_ld_acquire(const unsigned long long* p) {
-  unsigned long long v;
-  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
+// one replica's energy of a round: (round + 1) << 32 | int32 energy, a single-copy-atomic word
+__device__ __forceinline__ void gms_st_word(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
-__device__ __forceinline__ void gms_st_release(unsigned long long* p, unsigned long long v) {
-  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+__device__ __forceinline__ unsigned long long gms_ld_word(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
 }
 
 // bit-sliced add of one input word into the 3-bit counters (k0 + 2 k1 + 4 k2 per bit, <= 7 inputs)
@@ -273,9 +276,8 @@ __global__ void __launch_bounds__(kGmsThreads, 1) gms_run_kernel(const GmsArgs a
       if (better) ebest = ecur;
       const unsigned int mask = __ballot_sync(0xffffffffu, better);
       if (tid == 0) *imp = mask;
-      const size_t at = (size_t)(rg & 1) * R + 32 * w + tid;
-      __stcg(a.pub + at, ecur);
-      gms_st_release(a.tags + at, (unsigned long long)rg + 1ull);
+      unsigned long long* pw = reinterpret_cast<unsigned long long*>(a.pub) + (size_t)(rg & 1) * R;
+      gms_st_word(pw + 32 * w + tid, ((unsigned long long)(uint32_t)(rg + 1) << 32) | (uint32_t)(int32_t)ecur);
     }
     __syncthreads();
     {
@@ -285,52 +287,55 @@ __global__ void __launch_bounds__(kGmsThreads, 1) gms_run_kernel(const GmsArgs a
         for (int p = tid; p < n_pos; p += B) bw[p] = (bw[p] & ~mk) | (sw[p] & mk);
       }
     }
-    if (tid < 32) {
-      // gather every slot's energy of this round (W CTAs), then the exchange step
-      int bad = 0;
-      const unsigned long long want = (unsigned long long)rg + 1ull;
-      for (int s = tid; s < R && !bad; s += 32) {
-        const size_t at = (size_t)(rg & 1) * R + s;
-        if (gms_ld_acquire(a.tags + at) < want) {
+    {
+      // gather every slot's energy of this round (W CTAs), all threads, bounded waits
+      const unsigned long long* pw = reinterpret_cast<const unsigned long long*>(a.pub) + (size_t)(rg & 1) * R;
+      const uint32_t tag = (uint32_t)(rg + 1);
+      for (int s = tid; s < R; s += B) {
+        unsigned long long v = gms_ld_word(pw + s);
+        if ((uint32_t)(v >> 32) != tag) {
           const unsigned long long t0 = gms_now();
-          while (gms_ld_acquire(a.tags + at) < want) {
+          bool bad = false;
+          while ((uint32_t)((v = gms_ld_word(pw + s)) >> 32) != tag) {
             if (*abort_flag) {
-              bad = 1;
+              bad = true;
               break;
             }
             if (gms_now() - t0 > (unsigned long long)a.timeout_ns) {
               *abort_flag = 1;
               atomicExch(a.err, DRIFT_PT_ETIMEOUT);
-              bad = 1;
+              bad = true;
               break;
             }
           }
+          if (bad) break;
         }
-        if (!bad) eall[s] = __ldcg(a.pub + at);
+        eall[s] = (long long)(int32_t)(uint32_t)v;
       }
-      if (!__any_sync(0xffffffffu, bad)) {
-        __syncwarp();
-        const int parity = (int)(rg & 1);
-        for (int rr = parity + 2 * tid; rr + 1 < R; rr += 64) {
-          const int sa = slot_sm[rr], sb = slot_sm[rr + 1];
-          const double dlt = d_mul(d_sub(a.betas[rr], a.betas[rr + 1]), (double)(eall[sa] - eall[sb]));
-          bool acc = dlt >= 0.0;
-          if (!acc) {
-            const U4 u = philox(U4{(uint32_t)rr, (uint32_t)rg, (uint32_t)((unsigned long long)rg >> 32),
-                                   ctr3(kTagSwap, a.inst)},
-                                a.k0, a.k1);
-            acc = uniform53(u.x, u.y) < exp_neg_d(dlt);
-          }
-          if (w == 0) {
-            stats[2 * rr] += 1;
-            stats[2 * rr + 1] += acc ? 1 : 0;
-          }
-          if (acc) {
-            slot_sm[rr] = sb;
-            slot_sm[rr + 1] = sa;
-            rung_sm[sa] = rr + 1;
-            rung_sm[sb] = rr;
-          }
+    }
+    __syncthreads();
+    if (tid < 32 && !*abort_flag) {
+      // the exchange step, identical in every CTA
+      const int parity = (int)(rg & 1);
+      for (int rr = parity + 2 * tid; rr + 1 < R; rr += 64) {
+        const int sa = slot_sm[rr], sb = slot_sm[rr + 1];
+        const double dlt = d_mul(d_sub(a.betas[rr], a.betas[rr + 1]), (double)(eall[sa] - eall[sb]));
+        bool acc = dlt >= 0.0;
+        if (!acc) {
+          const U4 u = philox(U4{(uint32_t)rr, (uint32_t)rg, (uint32_t)((unsigned long long)rg >> 32),
+                                 ctr3(kTagSwap, a.inst)},
+                              a.k0, a.k1);
+          acc = uniform53(u.x, u.y) < exp_neg_d(dlt);
+        }
+        if (w == 0) {
+          stats[2 * rr] += 1;
+          stats[2 * rr + 1] += acc ? 1 : 0;
+        }
+        if (acc) {
+          slot_sm[rr] = sb;
+          slot_sm[rr + 1] = sa;
+          rung_sm[sa] = rr + 1;
+          rung_sm[sb] = rr;
         }
       }
     }
@@ -763,66 +768,69 @@ __global__ void __launch_bounds__(kGmcMaxThreads, 1) gmc_run_kernel(const GmsArg
     // ---- round end: cluster energy counts, publication and exchange on rank 0 ----
     flush_counts(cs, cnt);
     gmc_sync_smem();
-    if (rank == 0 && tid < 32) {
-      unsigned int tot = 0u;
-      for (int r = 0; r < C; ++r) tot += gmc_ld(gmc_map(gmc_saddr(cnt + tid), (uint32_t)r));
-      ecur = 2 * (long long)tot - a.n_bonds;
-      const bool better = ecur < ebest;
-      if (better) ebest = ecur;
-      const unsigned int mask = __ballot_sync(0xffffffffu, better);
+    if (rank == 0) {
       const uint32_t tag = (uint32_t)(rg + 1);
       unsigned long long* pub = reinterpret_cast<unsigned long long*>(a.pub) + (size_t)(rg & 1) * R;
-      gmc_st_pub(pub + 32 * w + tid, ((unsigned long long)tag << 32) | (uint32_t)(int32_t)ecur);
-      int bad = 0;
-      for (int s = tid; s < R && !bad; s += 32) {
+      if (tid < 32) {
+        unsigned int tot = 0u;
+        for (int r = 0; r < C; ++r) tot += gmc_ld(gmc_map(gmc_saddr(cnt + tid), (uint32_t)r));
+        ecur = 2 * (long long)tot - a.n_bonds;
+        const bool better = ecur < ebest;
+        if (better) ebest = ecur;
+        const unsigned int mask = __ballot_sync(0xffffffffu, better);
+        if (tid == 0) bcast[0] = (int)mask;
+        gmc_st_pub(pub + 32 * w + tid, ((unsigned long long)tag << 32) | (uint32_t)(int32_t)ecur);
+      }
+      // every slot's energy of this round, gathered by all of rank 0's threads (bounded waits)
+      for (int s = tid; s < R; s += B) {
         unsigned long long v = gmc_ld_pub(pub + s);
         if ((uint32_t)(v >> 32) != tag) {
           const unsigned long long t0 = gms_now();
+          bool bad = false;
           while ((uint32_t)((v = gmc_ld_pub(pub + s)) >> 32) != tag) {
             if (*abort_flag) {
-              bad = 1;
+              bad = true;
               break;
             }
             if (gms_now() - t0 > (unsigned long long)a.timeout_ns) {
               *abort_flag = 1;
               atomicExch(a.err, DRIFT_PT_ETIMEOUT);
-              bad = 1;
+              bad = true;
               break;
             }
           }
+          if (bad) break;
         }
-        if (!bad) eall[s] = (long long)(int32_t)(uint32_t)v;
+        eall[s] = (long long)(int32_t)(uint32_t)v;
       }
-      const bool any_bad = __any_sync(0xffffffffu, bad);
-      if (!any_bad) {
+      __syncthreads();  // rank is the same for every thread of a CTA
+      if (tid < 32) {
+        if (!*abort_flag) {
+          const int parity = (int)(rg & 1);
+          for (int rr = parity + 2 * tid; rr + 1 < R; rr += 64) {
+            const int sa = slot_sm[rr], sb = slot_sm[rr + 1];
+            const double dlt = d_mul(d_sub(a.betas[rr], a.betas[rr + 1]), (double)(eall[sa] - eall[sb]));
+            bool acc = dlt >= 0.0;
+            if (!acc) {
+              const U4 uu = philox(U4{(uint32_t)rr, (uint32_t)rg, (uint32_t)((unsigned long long)rg >> 32),
+                                      ctr3(kTagSwap, a.inst)},
+                                   a.k0, a.k1);
+              acc = uniform53(uu.x, uu.y) < exp_neg_d(dlt);
+            }
+            if (w == 0) {
+              stats[2 * rr] += 1;
+              stats[2 * rr + 1] += acc ? 1 : 0;
+            }
+            if (acc) {
+              slot_sm[rr] = sb;
+              slot_sm[rr + 1] = sa;
+              rung_sm[sa] = rr + 1;
+              rung_sm[sb] = rr;
+            }
+          }
+        }
         __syncwarp();
-        const int parity = (int)(rg & 1);
-        for (int rr = parity + 2 * tid; rr + 1 < R; rr += 64) {
-          const int sa = slot_sm[rr], sb = slot_sm[rr + 1];
-          const double dlt = d_mul(d_sub(a.betas[rr], a.betas[rr + 1]), (double)(eall[sa] - eall[sb]));
-          bool acc = dlt >= 0.0;
-          if (!acc) {
-            const U4 uu = philox(U4{(uint32_t)rr, (uint32_t)rg, (uint32_t)((unsigned long long)rg >> 32),
-                                    ctr3(kTagSwap, a.inst)},
-                                 a.k0, a.k1);
-            acc = uniform53(uu.x, uu.y) < exp_neg_d(dlt);
-          }
-          if (w == 0) {
-            stats[2 * rr] += 1;
-            stats[2 * rr + 1] += acc ? 1 : 0;
-          }
-          if (acc) {
-            slot_sm[rr] = sb;
-            slot_sm[rr + 1] = sa;
-            rung_sm[sa] = rr + 1;
-            rung_sm[sb] = rr;
-          }
-        }
-      }
-      __syncwarp();
-      if (tid == 0) {
-        bcast[0] = (int)mask;
-        bcast[1] = any_bad || *abort_flag ? 1 : 0;
+        if (tid == 0) bcast[1] = *abort_flag ? 1 : 0;
       }
     }
     gmc_sync_smem();
@@ -885,6 +893,7 @@ int gms_args(const DriftPtGmsProblem* p, const DriftPtGmsRunArgs* r, DriftPtGmsS
   if (!p->color_ptr || !p->ell_nbr || !p->degree || !p->jneg) return set_error(DRIFT_PT_EINVAL, "gms: problem arrays missing");
   if (p->max_class < 1 || p->max_class > p->n) return set_error(DRIFT_PT_EINVAL, "gms: max_class must be in 1..n");
   if (r->n_words < 1 || r->n_words > 64) return set_error(DRIFT_PT_EINVAL, "gms: n_words must be in 1..64");
+  if (p->n_bonds >= (1ll << 31)) return set_error(DRIFT_PT_EUNSUPPORTED, "gms: 2^31 or more bonds");
   if (r->instance > kMaxInstance) return set_error(DRIFT_PT_EINVAL, "gms: instance >= 2^24");
   if (!s->words || !s->best_words || !s->energy || !s->best_energy || !s->rung_of_slot || !s->slot_of_rung ||
       !s->swap_tried || !s->swap_accepted)
