@@ -601,7 +601,8 @@ DRIFT_PT_API int drift_pt_made_mh(const DriftPtSkProblem* problem, const DriftPt
  * from the networks, their sample counts, their output buffers x[g] ([counts[g]][n_g] int8, site
  * order) and logq[g] ([counts[g]] fp32), and a mode (0: draw, 1: evaluate the given x). Each
  * drift_pt_made_group_run then runs network g exactly as drift_pt_made_sample would with
- * stream_id[g] + stream_add, on blocks (., g) of one launch; max_* bound every network's sizes. */
+ * stream_id[g] + stream_add, on blocks (., g) of one launch; max_* bound every network's sizes.
+ * No counterpart in the reference (learned proposals are this engine's own). */
 DRIFT_PT_API int drift_pt_made_group_bytes(int32_t n_nets, size_t* bytes);
 DRIFT_PT_API int drift_pt_made_group_fill(int32_t n_nets, const DriftPtMadeNet* nets, const int32_t* counts,
                                           int32_t mode, int8_t* const* x, float* const* logq, uint64_t seed,
