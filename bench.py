@@ -1159,6 +1159,59 @@ def bench_ea2d_batch(args):
         dist.destroy_process_group()
 
 
+def call_latency(args):
+    """Wall time of one small solve()-style call (the reference's default PT settings: 16 replicas,
+    T 0.1-5, 300 rounds x 5 sweeps) on 20- and 40-spin +-1 instances, three ways: the in-process
+    drop-in parallel_tempering_gpu, the reference's own GPU engine behind its subprocess + problem
+    file boundary (drift/gpu.py:83-114; the binary built from cuda/ising_pt.cu into oracle/_ref),
+    and this engine's ising_pt command behind the same boundary. Median over `steps` calls after
+    `warmup`; the subprocess rows include process start and CUDA context creation, as the
+    reference's path does on every call."""
+    import tempfile
+
+    import torch
+
+    import oracle
+    from drift_b200.build import CLI_PATH
+    from drift_b200.gpu import parallel_tempering_gpu
+    from drift_b200.instances import gnp_pm
+    from drift_b200.problem_io import read_result, write_problem
+
+    torch.cuda.init()
+    kw = dict(n_replicas=16, T_min=0.1, T_max=5.0, n_rounds=300, sweeps_per_round=5)
+    out = {"metric": "seconds per solve() call", "unit": "s", "higher_is_better": False, "data": "synthetic",
+           "config": {"workload": "G(n, p) +-1 instances, n = 20 and 40; 16 replicas, T 0.1-5, 300 rounds x 5 sweeps",
+                      "steps": args.steps, "warmup": args.warmup, "statistic": "median"}, "rows": []}
+
+    def median_time(fn):
+        for _ in range(args.warmup):
+            fn()
+        ts = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            fn()
+            ts.append(time.perf_counter() - t0)
+        return float(np.median(ts))
+
+    with tempfile.TemporaryDirectory() as d:
+        prob, res = os.path.join(d, "problem.bin"), os.path.join(d, "result.bin")
+        for n, pp in ((20, 0.3), (40, 0.15)):
+            model = gnp_pm(n, pp, 7)
+            row = {"n": n, "drop_in_s": median_time(lambda: parallel_tempering_gpu(model, seed=1, **kw))}
+
+            def through_files(binary):
+                write_problem(prob, model, seed=1, **kw)
+                r = subprocess.run([binary, prob, res], capture_output=True, text=True)
+                if r.returncode != 0:
+                    raise RuntimeError(r.stderr[-300:])
+                read_result(res, n)
+
+            for key, binary in (("reference_subprocess_s", oracle.REF_BIN), ("ising_pt_command_s", CLI_PATH)):
+                row[key] = median_time(lambda: through_files(binary)) if os.path.exists(binary) else None
+            out["rows"].append(row)
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1182,8 +1235,12 @@ def main():
                     help="batched neural PT: plain rounds that collect each network's training set (8 per round)")
     ap.add_argument("--rounds", type=int, default=0,
                     help="override the rounds per step (profiling of a short case; the line then says so)")
+    ap.add_argument("--call-latency", action="store_true",
+                    help="time one small solve()-style call: in-process drop-in vs the subprocess + file boundary")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.call_latency:
+        call_latency(args)
+    elif args.impl == "reference":
         bench_reference(args)
     elif args.impl == "reference-gpu":
         bench_reference_gpu(args)
