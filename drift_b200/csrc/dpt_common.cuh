@@ -37,15 +37,11 @@ constexpr uint32_t kPhiloxM1 = 0xCD9E8D57u;  // multiplier applied to counter wo
 constexpr uint32_t kPhiloxW0 = 0x9E3779B9u;  // Weyl increment of key word 0 (golden ratio)
 constexpr uint32_t kPhiloxW1 = 0xBB67AE85u;  // Weyl increment of key word 1 (sqrt 3 - 1)
 
+// one widening multiply: on the device a single 32x32->64 multiply-add gives both halves
 DPT_HD void mulhilo32(uint32_t a, uint32_t b, uint32_t& hi, uint32_t& lo) {
-#if defined(__CUDA_ARCH__)
-  lo = a * b;
-  hi = __umulhi(a, b);
-#else
-  uint64_t p = (uint64_t)a * (uint64_t)b;
+  const uint64_t p = (uint64_t)a * (uint64_t)b;
   lo = (uint32_t)p;
   hi = (uint32_t)(p >> 32);
-#endif
 }
 
 // Ten rounds; the key is bumped between rounds (the bump after the last round is never used).
