@@ -67,26 +67,17 @@ static void philox_w(uint32_t a, uint32_t b, uint32_t c, uint32_t d, uint32_t k0
 /* exp(x), x <= 0: x = n ln2 + r, e^r by its Taylor series (Horner, fused multiply-add),        */
 /* result scaled by 2^n. Compiled with -ffp-contract=off so every other operation rounds once. */
 /* ------------------------------------------------------------------------------------------ */
-static double taylor_inv_fact_d[14];
-static float taylor_inv_fact_f[8];
-
-static void init_taylor(void) {
-  static int done = 0;
-  if (done) return;
-  /* 1/k! as the correctly rounded double / float of the exact rational (hex literals of the
-   * rounded values; 1/0! = 1/1! = 1, 1/2! = 0.5 are exact). */
-  const double d[14] = {1.0, 1.0, 0.5, 0x1.5555555555555p-3, 0x1.5555555555555p-5, 0x1.1111111111111p-7,
-                        0x1.6c16c16c16c17p-10, 0x1.a01a01a01a01ap-13, 0x1.a01a01a01a01ap-16,
-                        0x1.71de3a556c734p-19, 0x1.27e4fb7789f5cp-22, 0x1.ae64567f544e4p-26,
-                        0x1.1eed8eff8d898p-29, 0x1.6124613a86d09p-33};
-  const float f[8] = {1.0f, 1.0f, 0.5f, 0x1.555556p-3f, 0x1.555556p-5f, 0x1.111112p-7f, 0x1.6c16c2p-10f, 0x1.a01a02p-13f};
-  memcpy(taylor_inv_fact_d, d, sizeof d);
-  memcpy(taylor_inv_fact_f, f, sizeof f);
-  done = 1;
-}
+/* 1/k! as the correctly rounded double / float of the exact rational (hex literals of the rounded
+ * values; 1/0! = 1/1! = 1, 1/2! = 0.5 are exact). Constant tables: the replicas call the
+ * exponentials from several threads at once, so nothing here is initialised at run time. */
+static const double taylor_inv_fact_d[14] = {1.0, 1.0, 0.5, 0x1.5555555555555p-3, 0x1.5555555555555p-5,
+                                             0x1.1111111111111p-7, 0x1.6c16c16c16c17p-10, 0x1.a01a01a01a01ap-13,
+                                             0x1.a01a01a01a01ap-16, 0x1.71de3a556c734p-19, 0x1.27e4fb7789f5cp-22,
+                                             0x1.ae64567f544e4p-26, 0x1.1eed8eff8d898p-29, 0x1.6124613a86d09p-33};
+static const float taylor_inv_fact_f[8] = {1.0f, 1.0f, 0.5f, 0x1.555556p-3f, 0x1.555556p-5f, 0x1.111112p-7f,
+                                           0x1.6c16c2p-10f, 0x1.a01a02p-13f};
 
 double oracle_exp_neg_d(double x) {
-  init_taylor();
   if (!(x <= 0.0)) return 1.0;
   if (x < -708.0) return 0.0;
   double n = rint(x * 0x1.71547652b82fep+0);
@@ -101,7 +92,6 @@ double oracle_exp_neg_d(double x) {
 }
 
 float oracle_exp_neg_f(float x) {
-  init_taylor();
   if (!(x <= 0.0f)) return 1.0f;
   if (x < -87.0f) return 0.0f;
   float n = rintf(x * 0x1.715476p+0f);

@@ -185,6 +185,41 @@ def test_oracle_thread_count_does_not_change_results():
         assert np.array_equal(getattr(a, f), getattr(b, f)), f
 
 
+_FRESH_PROCESS_CHAIN = """
+import hashlib, sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+import oracle
+rng = np.random.default_rng(11)
+n, m = 3000, 9000
+e = rng.integers(0, n, size=(m, 2))
+e = e[e[:, 0] != e[:, 1]]
+J = np.zeros((n, n), np.float32)
+J[e[:, 0], e[:, 1]] = rng.standard_normal(len(e)).astype(np.float32)
+J = np.triu(J, 1); J = J + J.T
+row_ptr = np.concatenate([[0], np.cumsum((J != 0).sum(1))]).astype(np.int32)
+col_idx = np.nonzero(J)[1].astype(np.int32)
+w = J[J != 0].astype(np.float32)
+h = (0.1 * rng.standard_normal(n)).astype(np.float32)
+_, _, cp, cs = oracle.greedy_coloring(n, row_ptr, col_idx)
+prob = oracle.OracleProblem(n, row_ptr, col_idx, w, h, cp, cs, integer_path=False)
+st = oracle.pt_run(prob, 1.0 / np.geomspace(3.0, 0.1, 8), n_rounds=2, sweeps_per_round=2, seed=5, threads=8)
+print(hashlib.sha256(st.spins.tobytes() + st.energy.tobytes()).hexdigest())
+"""
+
+
+def test_oracle_fp32_chain_is_the_same_in_fresh_processes():
+    """The first exponentials of a process are evaluated by several replica threads at once; the
+    chain must not depend on which thread gets there first (run in new processes, 8 threads)."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    outs = {subprocess.run([sys.executable, "-c", _FRESH_PROCESS_CHAIN, root], capture_output=True, text=True,
+                           check=True, timeout=120).stdout.strip() for _ in range(10)}
+    assert len(outs) == 1, outs
+
+
 def test_oracle_swap_rate_matches_reference_cpu_statistically(reference_instances):
     """Equilibrium swap acceptance depends only on the Boltzmann energy distributions, so the
     colour-ordered chain and the reference's random-site chain agree within sampling noise."""
