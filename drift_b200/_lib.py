@@ -64,7 +64,7 @@ class DeviceState(C.Structure):
 
 class RunArgs(C.Structure):
     _fields_ = [("n_replicas", C.c_int32), ("n_rounds", C.c_int32), ("sweeps_per_round", C.c_int32),
-                ("reserved0", C.c_int32), ("round_offset", C.c_int64), ("seed", C.c_uint64),
+                ("round_sync", C.c_int32), ("round_offset", C.c_int64), ("seed", C.c_uint64),
                 ("instance", C.c_uint32), ("replicas_per_cta", C.c_int32), ("threads_per_cta", C.c_int32),
                 ("positions_per_item", C.c_int32), ("betas", vp), ("thresholds", vp), ("timeout_s", C.c_double)]
 

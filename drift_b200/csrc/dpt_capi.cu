@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <mutex>
 #include <utility>
 #include <vector>
@@ -164,8 +165,50 @@ namespace {
 
 struct LaunchPlan {
   int rpc, threads, in_smem, grid, p;
+  int cluster;  // > 0: the grid is one cluster of this many CTAs
   size_t smem;
 };
+
+constexpr int kMaxCluster = 16;
+
+// Can `C` CTAs of `threads` threads and `smem` bytes run as one cluster on this device? The answer
+// is cached per kernel, device and shape (the occupancy query costs more than a small run).
+int cluster_fits(const void* fn, int C, int threads, size_t smem, bool* ok) {
+  *ok = false;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  static std::mutex mu;
+  static std::map<std::tuple<const void*, int, int, int, size_t>, bool> known;
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_tuple(fn, dev, C, threads, smem);
+  const auto it = known.find(key);
+  if (it != known.end()) {
+    *ok = it->second;
+    return DRIFT_PT_OK;
+  }
+  if (C > 8) {
+    const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return cuda_fail(e, "cluster size attribute");
+  }
+  cudaLaunchConfig_t cfg;
+  std::memset(&cfg, 0, sizeof cfg);
+  cfg.gridDim = dim3(C);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  const cudaError_t e = cudaOccupancyMaxActiveClusters(&n, fn, &cfg);
+  if (e != cudaSuccess) return cuda_fail(e, "cluster occupancy query");
+  *ok = n >= 1;
+  known[key] = *ok;
+  return DRIFT_PT_OK;
+}
 
 int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPlan* lp) {
   DeviceInfo di;
@@ -173,8 +216,9 @@ int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPl
   if (rc) return rc;
   const int R = r->n_replicas;
   const int ip = p->integer_path;
-  auto total = [&](int rpc, bool ell, int threads) {
-    return smem_layout(p->n_pos, rpc, R, p->max_field, p->n_colors, p->n_slices, p->n_ell, ip != 0, ell, threads)
+  auto total = [&](int rpc, bool ell, int threads, bool cluster = false) {
+    return smem_layout(p->n_pos, rpc, R, p->max_field, p->n_colors, p->n_slices, p->n_ell, ip != 0, ell, threads,
+                       cluster)
         .total;
   };
   // positions per item (8, 4 or 2; the fp32 path always uses 8)
@@ -197,6 +241,60 @@ int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPl
     }
     return rpc * tps <= kMaxThreads ? tps : 0;
   };
+  auto shape_ok = [&](int rpc_, int threads_) {
+    const int tps = threads_ / rpc_;
+    const bool pow2 = tps > 0 && (tps & (tps - 1)) == 0;
+    return threads_ >= 32 && threads_ <= kMaxThreads && threads_ % 32 == 0 && threads_ % rpc_ == 0 &&
+           (tps % 32 == 0 || (tps < 32 && pow2));
+  };
+  // Round synchronisation. One cluster holding the whole ladder exchanges each round's energies
+  // through distributed shared memory behind one hardware barrier; it needs the ladder in at most
+  // 16 CTAs and the coupling table in shared memory. Chosen automatically when every slot keeps the
+  // threads it would have alone (one pass over each colour class), which is where the round end is
+  // a large share of the round; otherwise the grid form, which meets at a bounded barrier in global
+  // memory.
+  const int mode = r->round_sync;
+  if (mode < 0 || mode > 2) return set_error(DRIFT_PT_EINVAL, "round_sync must be 0 (auto), 1 (grid) or 2 (cluster)");
+  lp->cluster = 0;
+  if (mode != 1 && R > 1) {
+    int rc_c = r->replicas_per_cta;
+    if (rc_c <= 0) {
+      rc_c = 1;
+      while ((R + rc_c - 1) / rc_c > kMaxCluster) rc_c *= 2;
+    }
+    rc_c = std::min(rc_c, R);
+    const int C = (R + rc_c - 1) / rc_c;
+    int thr_c = r->threads_per_cta;
+    bool ok = C >= 2 && C <= kMaxCluster;
+    if (ok && thr_c <= 0) {
+      const int t = pick_tps(rc_c);
+      ok = t > 0 && (mode == 2 || t == pick_tps(1));
+      thr_c = rc_c * t;
+    }
+    ok = ok && shape_ok(rc_c, thr_c) && total(rc_c, true, thr_c, true) <= (size_t)di.max_smem_optin;
+    if (ok) {
+      const void* fn = run_kernel_ptr(ip, 1, p->max_width, p->min_width, p->has_field, P, 1);
+      const size_t smem = total(rc_c, true, thr_c, true);
+      int per_sm = 0;
+      rc = prepare_kernel(fn, thr_c, smem, &per_sm);
+      if (rc) return rc;
+      rc = cluster_fits(fn, C, thr_c, smem, &ok);
+      if (rc) return rc;
+      if (ok) {
+        lp->rpc = rc_c;
+        lp->p = P;
+        lp->threads = thr_c;
+        lp->in_smem = 1;
+        lp->grid = C;
+        lp->cluster = C;
+        lp->smem = smem;
+        return DRIFT_PT_OK;
+      }
+    }
+    if (mode == 2)
+      return set_error(DRIFT_PT_EUNSUPPORTED, "round_sync = 2: the ladder does not fit one cluster of at most %d CTAs "
+                       "with its coupling table in shared memory", kMaxCluster);
+  }
   int rpc = r->replicas_per_cta;
   if (rpc <= 0) {
     // One replica per CTA, as many CTAs as SMs allow. Measured on B200 from 24 to 576 spins,
@@ -287,13 +385,20 @@ extern "C" int drift_pt_run(const DriftPtDeviceProblem* prob, const DriftPtRunAr
   cfg.dynamicSmemBytes = lp.smem;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeCooperative;
-  attr[0].val.cooperative = 1;
+  if (lp.cluster > 0) {
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = lp.cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+  } else {
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+  }
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   void* kargs[] = {&a};
   e = cudaLaunchKernelExC(&cfg, run_kernel_ptr(prob->integer_path, lp.in_smem, prob->max_width, prob->min_width,
-                                                prob->has_field, lp.p),
+                                                prob->has_field, lp.p, lp.cluster > 0 ? 1 : 0),
                           kargs);
   if (e != cudaSuccess) return cuda_fail(e, "pt_run_kernel launch");
   return DRIFT_PT_OK;

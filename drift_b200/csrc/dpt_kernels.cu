@@ -49,6 +49,32 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
   return v;
 }
 
+// Cluster form: the CTAs of one thread-block cluster hold the whole ladder. A round's energies stay
+// in each CTA's shared memory; one cluster barrier (each thread's shared-memory writes released at
+// cluster scope, an acquiring wait) orders them before the other CTAs read them.
+__device__ __forceinline__ void cl_arrive_smem() {
+  __syncwarp();  // the .aligned barrier wants the whole warp converged
+  asm volatile("fence.release.sync_restrict::shared::cta.cluster;\n\tbarrier.cluster.arrive.relaxed.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void cl_wait() {
+  __syncwarp();
+  asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void cl_sync_full() {
+  __syncwarp();
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ uint32_t cl_map(uint32_t saddr, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ long long cl_ld_s64(uint32_t caddr) {
+  long long v;
+  asm volatile("ld.shared::cluster.s64 %0, [%1];" : "=l"(v) : "r"(caddr) : "memory");
+  return v;
+}
+
 __device__ __forceinline__ int ld_relaxed_i32(const int* p) {
   int v;
   asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -60,13 +86,16 @@ __device__ __forceinline__ int ld_relaxed_i32(const int* p) {
 // [lo, hi) are computed but never flipped. All gathers of the item are issued before the
 // acceptance tests (W bounds the slice width at compile time; W = 0 walks it at run time).
 // ---------------------------------------------------------------------------------------------
-template <bool kInt, bool kInSmem, int W, bool kExactW, bool kField, int P>
+// kCluster: the grid is one cluster (CTA rank = blockIdx.x) and the round's energies are exchanged
+// through distributed shared memory behind one cluster barrier instead of global memory.
+template <bool kInt, bool kInSmem, int W, bool kExactW, bool kField, int P, bool kCluster>
 __global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelArgs a) {
   static_assert(P == 8 || (kInt && P == 4), "positions per item");
   constexpr int NB = kGroup / P;  // items per group
   unsigned char* smem = dpt_smem;
   const SmemLayout L = smem_layout(a.n_pos, a.rpc, a.R, a.F, a.n_colors, a.n_slices, a.n_ell, kInt, kInSmem,
-                                   (int)blockDim.x);
+                                   (int)blockDim.x, kCluster);
+  long long* cpub = reinterpret_cast<long long*>(smem + L.cpub);
   int8_t* sp = reinterpret_cast<int8_t*>(smem + L.spins);
   long long* eacc = reinterpret_cast<long long*>(smem + L.eacc);
   long long* ecur = reinterpret_cast<long long*>(smem + L.ecur);
@@ -197,7 +226,17 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelAr
         __syncthreads();
       }
     }
-    // ---- round end: reduce the energy change of each slot over its threads ----
+    // ---- round end ----
+    // The exchange lanes draw the swap uniform of their first pair now: it depends only on the pair
+    // and the round, so its latency hides behind the energy reduction.
+    const int parity = (int)(round & 1);
+    double u_first = 0.0;
+    if (tid < 32 && parity + 2 * tid + 1 < R) {
+      const U4 u = philox(U4{(uint32_t)(parity + 2 * tid), (uint32_t)round, (uint32_t)((unsigned long long)round >> 32),
+                             ctr3(kTagSwap, a.inst)}, a.k0, a.k1);
+      u_first = uniform53(u.x, u.y);
+    }
+    // reduce the energy change of each slot over its threads
     for (int off = seg >> 1; off > 0; off >>= 1) dacc += __shfl_xor_sync(0xffffffffu, dacc, off);
     if (lt % seg == 0) eacc[tid / seg] = dacc;
     __syncthreads();
@@ -208,7 +247,9 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelAr
       ecur[i] = e;
       imp[i] = (e < ebest[i]) ? 1 : 0;
       if (e < ebest[i]) ebest[i] = e;
-      if (gridDim.x > 1) {
+      if constexpr (kCluster) {
+        cpub[(round & 1) * a.rpc + i] = e;
+      } else if (gridDim.x > 1) {
         const size_t at = (size_t)(round & 1) * R + s0 + i;
         if (a.packed) {
           // energy and round tag in one single-copy-atomic word: no ordering between two words needed
@@ -221,7 +262,14 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelAr
         }
       }
     }
-    __syncthreads();
+    if constexpr (kCluster) {
+      // one cluster barrier publishes this round's energies to the other CTAs and, being a barrier
+      // of every thread of the cluster, orders this CTA's own round-end writes for all its threads
+      cl_arrive_smem();
+      cl_wait();
+    } else {
+      __syncthreads();
+    }
     {
       // copy the spins of every slot that reached a new best, all slots in one pass
       const int chunks = n_pos / 16;
@@ -230,7 +278,15 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelAr
       for (int i = tid; i < nloc * chunks; i += B)
         if (imp[i / chunks]) dst[i] = src[i];
     }
-    if (gridDim.x > 1) {
+    // cluster form: a slot's energy of this round, read from its owner's shared memory
+    const uint32_t cbase = kCluster ? (uint32_t)__cvta_generic_to_shared(cpub + (round & 1) * a.rpc) : 0u;
+    auto cl_energy = [&](int sl) {
+      const int o = sl / a.rpc;
+      return cl_ld_s64(cl_map(cbase + 8u * (uint32_t)(sl - o * a.rpc), (uint32_t)o));
+    };
+    if constexpr (kCluster) {
+      // nothing to gather: the exchange and history warps read the energies they use directly
+    } else if (gridDim.x > 1) {
       // gather every slot's energy of this round: poll its tag (acquire), then read the energy;
       // this is the only grid-wide synchronisation of the round, bounded by the timeout
       int abort_now = 0;
@@ -274,20 +330,25 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelAr
     } else {
       for (int i = tid; i < R; i += B) eall[i] = ecur[i];
     }
-    __syncthreads();
+    if constexpr (!kCluster) __syncthreads();
     // ---- exchange step: identical in every CTA (disjoint pairs, one lane per pair) ----
     if (tid < 32) {
-      const int parity = (int)(round & 1);
       for (int r = parity + 2 * tid; r + 1 < R; r += 64) {
         const int sa = slot_sm[r], sb = slot_sm[r + 1];
-        const long long de = eall[sa] - eall[sb];
+        long long de;
+        if constexpr (kCluster) de = cl_energy(sa) - cl_energy(sb);
+        else de = eall[sa] - eall[sb];
         const double ded = kInt ? (double)de : d_mul((double)de, kFloatEnergyScale);
         const double delta = d_mul(d_sub(beta_sm[r], beta_sm[r + 1]), ded);
         bool acc = delta >= 0.0;
         if (!acc) {
-          const U4 u = philox(U4{(uint32_t)r, (uint32_t)round, (uint32_t)((unsigned long long)round >> 32),
-                                 ctr3(kTagSwap, a.inst)}, a.k0, a.k1);
-          acc = uniform53(u.x, u.y) < exp_neg_d(delta);
+          double u = u_first;  // the first pair of the lane (r < 64)
+          if (r >= 64) {
+            const U4 w = philox(U4{(uint32_t)r, (uint32_t)round, (uint32_t)((unsigned long long)round >> 32),
+                                   ctr3(kTagSwap, a.inst)}, a.k0, a.k1);
+            u = uniform53(w.x, w.y);
+          }
+          acc = u < exp_neg_d(delta);
         }
         if (blockIdx.x == 0) {
           stats[2 * r] += 1;
@@ -300,15 +361,22 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelAr
           rung_sm[sb] = r;
         }
       }
-      if (blockIdx.x == 0 && a.best_hist) {
-        long long m = LLONG_MAX;
-        for (int i = tid; i < R; i += 32) m = min(m, eall[i]);
-        for (int off = 16; off > 0; off >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, off));
-        if (tid == 0) {
-          long long* rb = reinterpret_cast<long long*>(ctl + 2);
-          rb[0] = min(rb[0], m);
-          a.best_hist[j] = kInt ? (double)rb[0] : d_mul((double)rb[0], kFloatEnergyScale);
-        }
+    }
+    // best-energy history (CTA 0): warp 1 while warp 0 runs the exchange, or warp 0 after it
+    if (blockIdx.x == 0 && a.best_hist && (tid >> 5) == (B > 32 ? 1 : 0)) {
+      const int lane = tid & 31;
+      long long m = LLONG_MAX;
+      for (int i = lane; i < R; i += 32) {
+        long long e;
+        if constexpr (kCluster) e = cl_energy(i);
+        else e = eall[i];
+        m = min(m, e);
+      }
+      for (int off = 16; off > 0; off >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, off));
+      if (lane == 0) {
+        long long* rb = reinterpret_cast<long long*>(ctl + 2);
+        rb[0] = min(rb[0], m);
+        a.best_hist[j] = kInt ? (double)rb[0] : d_mul((double)rb[0], kFloatEnergyScale);
       }
     }
     __syncthreads();
@@ -319,6 +387,8 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelAr
   }
 
   // ---- write back ----
+  // cluster form: no CTA leaves while another may still read its last round's energies
+  if constexpr (kCluster) cl_sync_full();
   __syncthreads();
   {
     const int4* src = reinterpret_cast<const int4*>(sp);
@@ -491,36 +561,44 @@ cudaError_t launch_energy_fp64(const PtKernelArgs& a, int integer_path, const in
   return cudaGetLastError();
 }
 
-template <bool kInt, bool kInSmem, bool kField, int P>
+template <bool kInt, bool kInSmem, bool kField, int P, bool kCl>
 static const void* pick_w(int max_w, int min_w) {
   // uniform slice widths 3, 4 and 6 (regular graphs and lattices) get an exact-width gather;
   // otherwise widths up to 8 a predicated one, and wider slices a run-time loop
   if constexpr (kInSmem) {
-    if (min_w == max_w && max_w == 3) return (const void*)pt_run_kernel<kInt, kInSmem, 3, true, kField, P>;
-    if (min_w == max_w && max_w == 4) return (const void*)pt_run_kernel<kInt, kInSmem, 4, true, kField, P>;
-    if (min_w == max_w && max_w == 6) return (const void*)pt_run_kernel<kInt, kInSmem, 6, true, kField, P>;
+    if (min_w == max_w && max_w == 3) return (const void*)pt_run_kernel<kInt, kInSmem, 3, true, kField, P, kCl>;
+    if (min_w == max_w && max_w == 4) return (const void*)pt_run_kernel<kInt, kInSmem, 4, true, kField, P, kCl>;
+    if (min_w == max_w && max_w == 6) return (const void*)pt_run_kernel<kInt, kInSmem, 6, true, kField, P, kCl>;
   }
-  if (max_w >= 1 && max_w <= 8) return (const void*)pt_run_kernel<kInt, kInSmem, 8, false, kField, P>;
-  return (const void*)pt_run_kernel<kInt, kInSmem, 0, false, kField, P>;
+  if (max_w >= 1 && max_w <= 8) return (const void*)pt_run_kernel<kInt, kInSmem, 8, false, kField, P, kCl>;
+  return (const void*)pt_run_kernel<kInt, kInSmem, 0, false, kField, P, kCl>;
 }
 
-template <bool kInt, bool kInSmem, bool kField>
+template <bool kInt, bool kInSmem, bool kField, bool kCl>
 static const void* pick_p(int max_w, int min_w, int p) {
   if constexpr (kInt) {
-    if (p == 4) return pick_w<kInt, kInSmem, kField, 4>(max_w, min_w);
+    if (p == 4) return pick_w<kInt, kInSmem, kField, 4, kCl>(max_w, min_w);
   }
-  return pick_w<kInt, kInSmem, kField, 8>(max_w, min_w);
+  return pick_w<kInt, kInSmem, kField, 8, kCl>(max_w, min_w);
 }
 
+// The cluster form exists with the coupling table in shared memory only (small problems, where the
+// round end is a large share of the round).
 const void* run_kernel_ptr(int integer_path, int in_smem, int max_width, int min_width, int has_field,
-                           int positions_per_item) {
+                           int positions_per_item, int cluster) {
   const int p = positions_per_item, w = max_width, m = min_width;
-  if (integer_path) {
-    if (in_smem) return has_field ? pick_p<true, true, true>(w, m, p) : pick_p<true, true, false>(w, m, p);
-    return has_field ? pick_p<true, false, true>(w, m, p) : pick_p<true, false, false>(w, m, p);
+  if (cluster) {
+    if (!in_smem) return nullptr;
+    if (integer_path)
+      return has_field ? pick_p<true, true, true, true>(w, m, p) : pick_p<true, true, false, true>(w, m, p);
+    return has_field ? pick_p<false, true, true, true>(w, m, p) : pick_p<false, true, false, true>(w, m, p);
   }
-  if (in_smem) return has_field ? pick_p<false, true, true>(w, m, p) : pick_p<false, true, false>(w, m, p);
-  return has_field ? pick_p<false, false, true>(w, m, p) : pick_p<false, false, false>(w, m, p);
+  if (integer_path) {
+    if (in_smem) return has_field ? pick_p<true, true, true, false>(w, m, p) : pick_p<true, true, false, false>(w, m, p);
+    return has_field ? pick_p<true, false, true, false>(w, m, p) : pick_p<true, false, false, false>(w, m, p);
+  }
+  if (in_smem) return has_field ? pick_p<false, true, true, false>(w, m, p) : pick_p<false, true, false, false>(w, m, p);
+  return has_field ? pick_p<false, false, true, false>(w, m, p) : pick_p<false, false, false, false>(w, m, p);
 }
 
 }  // namespace dpt

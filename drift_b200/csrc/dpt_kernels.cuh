@@ -41,7 +41,7 @@ struct PtKernelArgs {
 
 struct SmemLayout {
   size_t spins, eacc, ecur, ebest, imp, eall, rung, slot, beta, nb, thr, stats, cptr, ctl;
-  size_t soff, nbr, w, h, total;
+  size_t soff, nbr, w, h, cpub, total;
 };
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
@@ -49,7 +49,8 @@ __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~(size_t
 // Byte offsets of every shared-memory array; the host sizes the launch with the same function.
 // Threads are bound to replica slots: `threads / rpc` threads per slot (a power of two below 32 or
 // a multiple of 32, so shuffle segments never straddle two slots). `eacc` holds one partial energy
-// change per shuffle segment.
+// change per shuffle segment. `cpub` (cluster form only) holds the slots' energies of the last two
+// rounds, read by the other CTAs of the cluster through distributed shared memory.
 __host__ __device__ inline int seg_width(int threads, int rpc) {
   const int tps = threads / rpc;
   return tps < 32 ? tps : 32;
@@ -57,7 +58,7 @@ __host__ __device__ inline int seg_width(int threads, int rpc) {
 
 __host__ __device__ inline SmemLayout smem_layout(int n_pos, int rpc, int R, int F, int n_colors, int n_slices,
                                                   long long n_ell, bool integer_path, bool ell_in_smem,
-                                                  int threads) {
+                                                  int threads, bool cluster = false) {
   SmemLayout L;
   size_t o = 0;
   L.spins = o; o = align16(o + (size_t)rpc * n_pos);
@@ -81,6 +82,7 @@ __host__ __device__ inline SmemLayout smem_layout(int n_pos, int rpc, int R, int
     L.w = o;    o = align16(o + (integer_path ? 0 : 4) * (size_t)n_ell);
     L.h = o;    o = align16(o + 4 * (size_t)n_pos);
   }
+  L.cpub = o;   o = align16(o + (cluster ? 16 * (size_t)rpc : 0));
   L.total = o;
   return L;
 }
@@ -89,6 +91,6 @@ cudaError_t launch_init(const PtKernelArgs& a, int integer_path, cudaStream_t st
 cudaError_t launch_energy_fp64(const PtKernelArgs& a, int integer_path, const int8_t* spins, int R, double* out,
                                cudaStream_t st);
 const void* run_kernel_ptr(int integer_path, int in_smem, int max_width, int min_width, int has_field,
-                           int positions_per_item);
+                           int positions_per_item, int cluster = 0);
 
 }  // namespace dpt

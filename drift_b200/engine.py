@@ -131,7 +131,7 @@ class PtEngine:
 
     def __init__(self, prob: DeviceProblem, betas, *, seed: int = 0, sweeps_per_round: int = 1, instance: int = 0,
                  replicas_per_cta: int = 0, threads_per_cta: int = 0, positions_per_item: int = 0,
-                 timeout_s: float = 10.0):
+                 timeout_s: float = 10.0, round_sync: int = 0):
         import torch
 
         self.torch = torch
@@ -147,6 +147,7 @@ class PtEngine:
             raise ValueError("sweeps_per_round must be >= 1")
         self.rpc, self.threads, self.timeout_s = int(replicas_per_cta), int(threads_per_cta), float(timeout_s)
         self.ppi = int(positions_per_item)
+        self.round_sync = int(round_sync)  # 0 auto, 1 grid barrier, 2 one cluster
         dev = prob.device
         L = _lib.load()
         self.d_betas = torch.from_numpy(self.betas).to(dev)
@@ -172,7 +173,7 @@ class PtEngine:
         self.history = None
 
     def _args(self, n_rounds: int) -> _lib.RunArgs:
-        return _lib.RunArgs(self.R, n_rounds, self.spr, 0, self.rounds_done, self.seed & 0xFFFFFFFFFFFFFFFF,
+        return _lib.RunArgs(self.R, n_rounds, self.spr, self.round_sync, self.rounds_done, self.seed & 0xFFFFFFFFFFFFFFFF,
                             self.instance, self.rpc, self.threads, self.ppi, self.d_betas.data_ptr(),
                             self.d_thr.data_ptr() if self.thr is not None else None, self.timeout_s)
 

@@ -155,7 +155,11 @@ typedef struct DriftPtRunArgs {
   int32_t n_replicas;        /* R (rungs = slots)                                           */
   int32_t n_rounds;          /* rounds in this call                                         */
   int32_t sweeps_per_round;  /* Metropolis sweeps between exchange steps                    */
-  int32_t reserved0;
+  int32_t round_sync;        /* how the CTAs meet at each round end: 0 = auto, 1 = grid
+                                (bounded barrier in global memory, any ladder), 2 = one
+                                thread-block cluster of at most 16 CTAs (energies through
+                                distributed shared memory; ladders that fit, coupling table in
+                                shared memory). The results do not depend on it.            */
   int64_t round_offset;      /* index of the first round (resume); sweeps are numbered
                                 round * sweeps_per_round + j                                */
   uint64_t seed;

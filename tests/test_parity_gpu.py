@@ -32,13 +32,13 @@ def oracle_problem(hp: HostProblem, integer_path: bool):
 
 
 def run_engine(model, betas, rounds, spr, seed, *, rpc=0, threads=0, ppi=0, instance=0, chunks=None,
-               integer_path=None):
+               integer_path=None, round_sync=0):
     import torch
 
     hp = HostProblem.from_model(model)
     prob = DeviceProblem(hp, integer_path=integer_path)
     eng = PtEngine(prob, betas, seed=seed, sweeps_per_round=spr, instance=instance, replicas_per_cta=rpc,
-                   threads_per_cta=threads, positions_per_item=ppi)
+                   threads_per_cta=threads, positions_per_item=ppi, round_sync=round_sync)
     eng.init()
     hist = torch.zeros(max(rounds, 1), dtype=torch.float64, device="cuda")
     done = 0
@@ -136,6 +136,37 @@ def test_results_do_not_depend_on_launch_shape(rpc, threads, ppi):
     hp, prob, eng, st, hist = run_engine(model, betas, rounds, spr, seed, rpc=rpc, threads=threads, ppi=ppi)
     ost = oracle.pt_run(oracle_problem(hp, True), betas, n_rounds=rounds, sweeps_per_round=spr, seed=seed, thr=eng.thr)
     assert_bit_exact(st, ost, hist, rounds)
+
+
+ROUND_SYNC_CASES = {
+    # name: (model factory, R, T range, rounds, sweeps_per_round, seed, replicas per CTA)
+    "ea2d_L16_R24": (lambda: ea_2d(16, 1), 24, (1 / 3.0, 10.0), 300, 1, 1, 0),
+    "glass_field_fp32_R20": (lambda: pm_spin_glass(14, 7, field=0.3), 20, (0.05, 5.0), 120, 2, 2, 0),
+    "ragged_257_R25_last_cta_short": (lambda: gnp_pm(257, 0.02, 4), 25, (0.2, 5.0), 60, 2, 3, 2),
+    "three_replicas": (lambda: maxcut_ising(random_graph(16, 0.5, 3)), 3, (0.2, 5.0), 80, 3, 4, 0),
+    "maxcut_2048_cluster_of_16": (lambda: maxcut_3regular(2048, 5), 16, (0.25, 5.0), 20, 2, 5, 1),
+    "er_fp32_R32_four_per_cta": (lambda: er_gaussian(600, 6, 7), 32, (1 / 3.0, 10.0), 30, 2, 6, 4),
+}
+
+
+@pytest.mark.parametrize("round_sync", [1, 2])
+@pytest.mark.parametrize("name", list(ROUND_SYNC_CASES))
+def test_round_sync_forms_match_oracle_bit_exact(name, round_sync):
+    """The grid form (bounded barrier in global memory) and the cluster form (energies through
+    distributed shared memory) run the same chain."""
+    make, R, (tmin, tmax), rounds, spr, seed, rpc = ROUND_SYNC_CASES[name]
+    model = make()
+    betas = geometric_betas(R, tmin, tmax)
+    hp, prob, eng, st, hist = run_engine(model, betas, rounds, spr, seed, rpc=rpc, round_sync=round_sync)
+    ost = oracle.pt_run(oracle_problem(hp, prob.integer_path), betas, n_rounds=rounds, sweeps_per_round=spr,
+                        seed=seed, thr=eng.thr)
+    assert_bit_exact(st, ost, hist, rounds)
+
+
+def test_cluster_form_refuses_a_ladder_that_does_not_fit():
+    betas = geometric_betas(64, 0.25, 5.0)
+    with pytest.raises(_lib.EngineError, match="one cluster"):
+        run_engine(maxcut_3regular(512, 1), betas, 2, 1, 0, rpc=1, round_sync=2)
 
 
 def test_fp32_path_launch_shapes_and_resume():
