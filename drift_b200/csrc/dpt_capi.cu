@@ -221,16 +221,16 @@ int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPl
                        cluster)
         .total;
   };
-  // positions per item (8, 4 or 2; the fp32 path always uses 8)
-  int P = r->positions_per_item;
-  if (P != 0 && P != 8 && P != 4) return set_error(DRIFT_PT_EINVAL, "positions_per_item must be 0, 4 or 8");
-  if (!ip) P = 8;
-  else if (P == 0) P = 4;  // measured faster on the integer path: shorter per-item dependency chains
+  // positions per item (8, 4 or 1; the fp32 path always uses 8); 0 = chosen below
+  const int P_user = r->positions_per_item;
+  if (P_user != 0 && P_user != 8 && P_user != 4 && P_user != 1)
+    return set_error(DRIFT_PT_EINVAL, "positions_per_item must be 0, 1, 4 or 8");
   // threads per slot: one per item of the largest colour class (32-group runs times 8/P
   // sub-blocks), as a power of two below 32 or a multiple of 32, with rpc * tps a multiple of 32
   // and at most kMaxThreads (0 = none)
-  const int want = ((p->max_class / kGroup + 2 + 31) / 32) * 32 * (kGroup / P);
-  auto pick_tps = [&](int rpc) -> int {
+  auto want_of = [&](int P_) { return ((p->max_class / kGroup + 2 + 31) / 32) * 32 * (kGroup / P_); };
+  auto pick_tps = [&](int rpc, int P_) -> int {
+    const int want = want_of(P_);
     int tps = 1;
     while (tps < 32 && tps < want) tps *= 2;
     if (tps >= 32) tps = ((want + 31) / 32) * 32;
@@ -241,22 +241,29 @@ int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPl
     }
     return rpc * tps <= kMaxThreads ? tps : 0;
   };
+  // one pass over each colour class: the slot gets a thread for every item of the largest class
+  auto one_pass = [&](int rpc, int P_) {
+    const int want = want_of(P_);
+    int full = 1;
+    while (full < 32 && full < want) full *= 2;
+    if (full >= 32) full = ((want + 31) / 32) * 32;
+    return pick_tps(rpc, P_) == full;
+  };
   auto shape_ok = [&](int rpc_, int threads_) {
     const int tps = threads_ / rpc_;
     const bool pow2 = tps > 0 && (tps & (tps - 1)) == 0;
     return threads_ >= 32 && threads_ <= kMaxThreads && threads_ % 32 == 0 && threads_ % rpc_ == 0 &&
            (tps % 32 == 0 || (tps < 32 && pow2));
   };
-  // Round synchronisation. One cluster holding the whole ladder exchanges each round's energies
-  // through distributed shared memory behind one hardware barrier; it needs the ladder in at most
-  // 16 CTAs and the coupling table in shared memory. Chosen automatically when every slot keeps the
-  // threads it would have alone (one pass over each colour class), which is where the round end is
-  // a large share of the round; otherwise the grid form, which meets at a bounded barrier in global
-  // memory.
   const int mode = r->round_sync;
   if (mode < 0 || mode > 2) return set_error(DRIFT_PT_EINVAL, "round_sync must be 0 (auto), 1 (grid) or 2 (cluster)");
   lp->cluster = 0;
-  if (mode != 1 && R > 1) {
+
+  // ---- the cluster form: the ladder in one cluster of at most 16 CTAs, coupling table in shared
+  // memory; a round's energies cross through distributed shared memory behind one barrier ----
+  auto try_cluster = [&](int P_, bool require_one_pass, bool* done) -> int {
+    *done = false;
+    if (R < 2) return DRIFT_PT_OK;
     int rc_c = r->replicas_per_cta;
     if (rc_c <= 0) {
       rc_c = 1;
@@ -267,78 +274,110 @@ int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPl
     int thr_c = r->threads_per_cta;
     bool ok = C >= 2 && C <= kMaxCluster;
     if (ok && thr_c <= 0) {
-      const int t = pick_tps(rc_c);
-      ok = t > 0 && (mode == 2 || t == pick_tps(1));
-      thr_c = rc_c * t;
+      ok = pick_tps(rc_c, P_) > 0 && (!require_one_pass || one_pass(rc_c, P_));
+      thr_c = rc_c * pick_tps(rc_c, P_);
     }
     ok = ok && shape_ok(rc_c, thr_c) && total(rc_c, true, thr_c, true) <= (size_t)di.max_smem_optin;
-    if (ok) {
-      const void* fn = run_kernel_ptr(ip, 1, p->max_width, p->min_width, p->has_field, P, 1);
-      const size_t smem = total(rc_c, true, thr_c, true);
-      int per_sm = 0;
-      rc = prepare_kernel(fn, thr_c, smem, &per_sm);
-      if (rc) return rc;
-      rc = cluster_fits(fn, C, thr_c, smem, &ok);
-      if (rc) return rc;
-      if (ok) {
-        lp->rpc = rc_c;
-        lp->p = P;
-        lp->threads = thr_c;
-        lp->in_smem = 1;
-        lp->grid = C;
-        lp->cluster = C;
-        lp->smem = smem;
-        return DRIFT_PT_OK;
-      }
+    if (!ok) return DRIFT_PT_OK;
+    const void* fn = run_kernel_ptr(ip, 1, p->max_width, p->min_width, p->has_field, P_, 1);
+    if (!fn) return DRIFT_PT_OK;
+    const size_t smem = total(rc_c, true, thr_c, true);
+    int per_sm = 0;
+    int rc2 = prepare_kernel(fn, thr_c, smem, &per_sm);
+    if (rc2) return rc2;
+    rc2 = cluster_fits(fn, C, thr_c, smem, &ok);
+    if (rc2 || !ok) return rc2;
+    lp->rpc = rc_c;
+    lp->p = P_;
+    lp->threads = thr_c;
+    lp->in_smem = 1;
+    lp->grid = C;
+    lp->cluster = C;
+    lp->smem = smem;
+    *done = true;
+    return DRIFT_PT_OK;
+  };
+
+  // ---- the grid form: any ladder; CTAs meet at a bounded barrier in global memory ----
+  auto plan_grid = [&](int P_) -> int {
+    int rpc = r->replicas_per_cta;
+    if (rpc <= 0) {
+      // One replica per CTA, as many CTAs as SMs allow. Measured on B200 from 24 to 576 spins,
+      // 16-64 replicas and 1-5 sweeps per round, this beats keeping every replica in one CTA
+      // (which needs no grid barrier) by 1.3x to 13x: the grid barrier costs less than running
+      // the replicas one after another on one SM.
+      rpc = 1;
+      while (rpc < R && (R + rpc - 1) / rpc > di.sm_count) rpc *= 2;
+      rpc = std::min(rpc, R);
+      while (rpc > 1 && pick_tps(rpc, P_) == 0) rpc /= 2;
     }
-    if (mode == 2)
-      return set_error(DRIFT_PT_EUNSUPPORTED, "round_sync = 2: the ladder does not fit one cluster of at most %d CTAs "
-                       "with its coupling table in shared memory", kMaxCluster);
-  }
-  int rpc = r->replicas_per_cta;
-  if (rpc <= 0) {
-    // One replica per CTA, as many CTAs as SMs allow. Measured on B200 from 24 to 576 spins,
-    // 16-64 replicas and 1-5 sweeps per round, this beats keeping every replica in one CTA
-    // (which needs no grid barrier) by 1.3x to 13x: the grid barrier costs less than running
-    // the replicas one after another on one SM.
-    rpc = 1;
-    while (rpc < R && (R + rpc - 1) / rpc > di.sm_count) rpc *= 2;
     rpc = std::min(rpc, R);
-    while (rpc > 1 && pick_tps(rpc) == 0) rpc /= 2;
-  }
-  rpc = std::min(rpc, R);
-  if ((R + rpc - 1) / rpc > 65535) return set_error(DRIFT_PT_EUNSUPPORTED, "too many CTAs");
-  int threads = r->threads_per_cta;
-  if (threads <= 0) {
-    const int tps = pick_tps(rpc);
-    if (tps == 0) return set_error(DRIFT_PT_EUNSUPPORTED, "no launch shape for %d replicas per CTA", rpc);
-    threads = rpc * tps;
-  }
-  {
-    const int tps = threads / rpc;
-    const bool pow2 = tps > 0 && (tps & (tps - 1)) == 0;
-    if (threads < 32 || threads > kMaxThreads || threads % 32 || threads % rpc || !(tps % 32 == 0 || (tps < 32 && pow2)))
+    if ((R + rpc - 1) / rpc > 65535) return set_error(DRIFT_PT_EUNSUPPORTED, "too many CTAs");
+    int threads = r->threads_per_cta;
+    if (threads <= 0) {
+      const int tps = pick_tps(rpc, P_);
+      if (tps == 0) return set_error(DRIFT_PT_EUNSUPPORTED, "no launch shape for %d replicas per CTA", rpc);
+      threads = rpc * tps;
+    }
+    if (!shape_ok(rpc, threads))
       return set_error(DRIFT_PT_EINVAL,
                        "threads_per_cta (%d) must be a multiple of 32 in [32, 512] and of replicas_per_cta (%d), "
                        "with threads/replica a power of two below 32 or a multiple of 32", threads, rpc);
+    if (total(rpc, false, threads) > (size_t)di.max_smem_optin)
+      return set_error(DRIFT_PT_EUNSUPPORTED, "replica state of %d x %d positions exceeds shared memory (%d B)", rpc,
+                       p->n_pos, di.max_smem_optin);
+    const bool in_smem = total(rpc, true, threads) <= (size_t)di.max_smem_optin;
+    lp->rpc = rpc;
+    lp->p = P_;
+    lp->threads = threads;
+    lp->in_smem = in_smem ? 1 : 0;
+    lp->grid = (R + rpc - 1) / rpc;
+    lp->smem = total(rpc, in_smem, threads);
+    const void* fn = run_kernel_ptr(ip, lp->in_smem, p->max_width, p->min_width, p->has_field, lp->p);
+    if (!fn)
+      return set_error(DRIFT_PT_EUNSUPPORTED, "one position per item needs the coupling table in shared memory");
+    int per_sm = 0;
+    const int rc2 = prepare_kernel(fn, threads, lp->smem, &per_sm);
+    if (rc2) return rc2;
+    if ((long long)per_sm * di.sm_count < lp->grid)
+      return set_error(DRIFT_PT_EUNSUPPORTED,
+                       "%d CTAs of %d threads / %zu B shared memory cannot be co-resident (%d per SM x %d SMs)",
+                       lp->grid, threads, lp->smem, per_sm, di.sm_count);
+    return DRIFT_PT_OK;
+  };
+
+  bool done = false;
+  if (!ip || P_user != 0 || r->replicas_per_cta > 0 || r->threads_per_cta > 0 || mode != 0) {
+    // the caller fixed part of the shape: the integer path defaults to 4 positions per item
+    const int P = !ip ? 8 : (P_user ? P_user : 4);
+    if (mode != 1) {
+      rc = try_cluster(P, mode == 0, &done);
+      if (rc || done) return rc;
+      if (mode == 2)
+        return set_error(DRIFT_PT_EUNSUPPORTED, "round_sync = 2: the ladder does not fit one cluster of at most %d "
+                         "CTAs with its coupling table in shared memory", kMaxCluster);
+    }
+    return plan_grid(P);
   }
-  if (total(rpc, false, threads) > (size_t)di.max_smem_optin)
-    return set_error(DRIFT_PT_EUNSUPPORTED, "replica state of %d x %d positions exceeds shared memory (%d B)", rpc,
-                     p->n_pos, di.max_smem_optin);
-  const bool in_smem = total(rpc, true, threads) <= (size_t)di.max_smem_optin;
-  lp->rpc = rpc;
-  lp->p = P;
-  lp->threads = threads;
-  lp->in_smem = in_smem ? 1 : 0;
-  lp->grid = (R + rpc - 1) / rpc;
-  lp->smem = total(rpc, in_smem, threads);
-  const void* fn = run_kernel_ptr(ip, lp->in_smem, p->max_width, p->min_width, p->has_field, lp->p);
-  int per_sm = 0;
-  rc = prepare_kernel(fn, threads, lp->smem, &per_sm);
-  if (rc) return rc;
-  if ((long long)per_sm * di.sm_count < lp->grid)
-    return set_error(DRIFT_PT_EUNSUPPORTED, "%d CTAs of %d threads / %zu B shared memory cannot be co-resident (%d per SM x %d SMs)",
-                     lp->grid, threads, lp->smem, per_sm, di.sm_count);
+  // Automatic shape on the integer path, from measurements on B200 (2-D EA L = 8, 16, 32 with 16-24
+  // replicas and G(n, p) n = 400 with 32, 1-4 sweeps per round):
+  //  * one position per item (the gather chain of a quarter of the positions) wins with one
+  //    replica per CTA when a class takes one pass, and loses with two replicas per CTA;
+  //  * the cluster form's round end is ~0.35 us shorter than the grid form's, a position per item
+  //    saves ~0.1 us per colour phase: with 16 replicas or fewer both are had at once; otherwise
+  //    the cluster (4 positions per item, 2+ replicas per CTA) wins below 4 colour phases per round
+  //    and one replica per CTA with a position per item from 4 phases on;
+  //  * 4 positions per item elsewhere (the largest classes, many replicas).
+  const bool p1_alone = one_pass(1, 1) && total(1, true, pick_tps(1, 1)) <= (size_t)di.max_smem_optin;
+  const long long phases = (long long)r->sweeps_per_round * p->n_colors;
+  if (p1_alone && R <= kMaxCluster) {
+    rc = try_cluster(1, true, &done);
+    if (rc || done) return rc;
+  }
+  if (p1_alone && R <= di.sm_count && phases >= 4) return plan_grid(1);
+  rc = try_cluster(4, true, &done);
+  if (rc || done) return rc;
+  return plan_grid(p1_alone && R <= di.sm_count ? 1 : 4);
   return DRIFT_PT_OK;
 }
 

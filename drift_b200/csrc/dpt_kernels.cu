@@ -90,7 +90,7 @@ __device__ __forceinline__ int ld_relaxed_i32(const int* p) {
 // through distributed shared memory behind one cluster barrier instead of global memory.
 template <bool kInt, bool kInSmem, int W, bool kExactW, bool kField, int P, bool kCluster>
 __global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelArgs a) {
-  static_assert(P == 8 || (kInt && P == 4), "positions per item");
+  static_assert(P == 8 || (kInt && (P == 4 || P == 1)), "positions per item");
   constexpr int NB = kGroup / P;  // items per group
   unsigned char* smem = dpt_smem;
   const SmemLayout L = smem_layout(a.n_pos, a.rpc, a.R, a.F, a.n_colors, a.n_slices, a.n_ell, kInt, kInSmem,
@@ -578,6 +578,10 @@ template <bool kInt, bool kInSmem, bool kField, bool kCl>
 static const void* pick_p(int max_w, int min_w, int p) {
   if constexpr (kInt) {
     if (p == 4) return pick_w<kInt, kInSmem, kField, 4, kCl>(max_w, min_w);
+    // one position per item: small problems only (coupling table in shared memory)
+    if constexpr (kInSmem)
+      if (p == 1) return pick_w<kInt, kInSmem, kField, 1, kCl>(max_w, min_w);
+    if (p == 1) return nullptr;
   }
   return pick_w<kInt, kInSmem, kField, 8, kCl>(max_w, min_w);
 }

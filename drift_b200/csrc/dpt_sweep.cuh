@@ -42,6 +42,7 @@ __device__ __forceinline__ int slice_off(const Tables& T, int S) {
 template <int P> struct SpinWord;
 template <> struct SpinWord<8> { using T = uint64_t; };
 template <> struct SpinWord<4> { using T = uint32_t; };
+template <> struct SpinWord<1> { using T = uint8_t; };
 
 // Bits i of the result: position 8g + q0 + i lies in the colour range [lo, hi).
 template <int P>
@@ -126,8 +127,19 @@ __device__ __forceinline__ int group_int(int g, int b, int lo, int hi, uint32_t 
     const int si = (int)(int8_t)(uint8_t)(s8 >> (8 * i));
     const int x = si * field[i];
     const uint32_t thr = lds_u32(thr_o + 4u * (uint32_t)x);
-    const uint32_t word = (P == 8) ? words[i >> 1] : (b ? words[2 + (i >> 1)] : words[i >> 1]);
-    const uint32_t prim = (word >> ((i & 1) * 16)) & 0xFFFFu;
+    // the 16-bit uniform of position q of the group: half q & 1 of word q >> 1
+    uint32_t word, sh;
+    if constexpr (P == 8) {
+      word = words[i >> 1];
+      sh = (uint32_t)(i & 1) * 16u;
+    } else if constexpr (P == 4) {
+      word = b ? words[2 + (i >> 1)] : words[i >> 1];
+      sh = (uint32_t)(i & 1) * 16u;
+    } else {
+      word = (q & 4) ? ((q & 2) ? words[3] : words[2]) : ((q & 2) ? words[1] : words[0]);
+      sh = (uint32_t)(q & 1) * 16u;
+    }
+    const uint32_t prim = (word >> sh) & 0xFFFFu;
     const uint32_t th = thr >> 16;
     const bool in = (inmask >> i) & 1u;
     bool acc = (x <= 0) | (prim < th);

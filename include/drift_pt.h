@@ -166,7 +166,8 @@ typedef struct DriftPtRunArgs {
   uint32_t instance;         /* stream id (< 2^24), distinct per independent chain set      */
   int32_t replicas_per_cta;  /* 0 = auto (autotuner)                                        */
   int32_t threads_per_cta;   /* 0 = auto; at most 512                                       */
-  int32_t positions_per_item;/* 8 or 4 spins per thread and phase (integer path); 0 = auto  */
+  int32_t positions_per_item;/* 8, 4 or 1 spins per thread and phase (4 and 1: integer path;
+                                1: coupling table in shared memory); 0 = auto               */
   const double* betas;       /* [R] inverse temperature of each rung                        */
   const uint32_t* thresholds;/* [R][F] integer path (from drift_pt_thresholds), else NULL   */
   double timeout_s;          /* bound on any in-kernel wait (0 = 10 s)                      */

@@ -163,6 +163,29 @@ def test_round_sync_forms_match_oracle_bit_exact(name, round_sync):
     assert_bit_exact(st, ost, hist, rounds)
 
 
+ONE_POSITION_CASES = {
+    # name: (model factory, R, T range, rounds, sweeps_per_round, seed)
+    "ea2d_L16_R24": (lambda: ea_2d(16, 1), 24, (1 / 3.0, 10.0), 200, 1, 1),
+    "ragged_25_R7": (lambda: ea_2d(5, 2), 7, (0.2, 5.0), 80, 3, 7),
+    "int_field_R9": (lambda: _pure_field(40, [-2.0, -1.0, 1.0, 2.0], 5), 9, (0.2, 5.0), 40, 2, 12),
+    "isolated_spins_R9": (_isolated_spins, 9, (0.2, 5.0), 60, 2, 8),
+    "ragged_257_R10": (lambda: gnp_pm(257, 0.02, 4), 10, (0.2, 5.0), 40, 2, 9),
+}
+
+
+@pytest.mark.parametrize("round_sync", [1, 2])
+@pytest.mark.parametrize("name", list(ONE_POSITION_CASES))
+def test_one_position_per_item_matches_oracle_bit_exact(name, round_sync):
+    make, R, (tmin, tmax), rounds, spr, seed = ONE_POSITION_CASES[name]
+    model = make()
+    betas = geometric_betas(R, tmin, tmax)
+    hp, prob, eng, st, hist = run_engine(model, betas, rounds, spr, seed, ppi=1, round_sync=round_sync)
+    assert prob.integer_path
+    ost = oracle.pt_run(oracle_problem(hp, True), betas, n_rounds=rounds, sweeps_per_round=spr, seed=seed,
+                        thr=eng.thr)
+    assert_bit_exact(st, ost, hist, rounds)
+
+
 def test_cluster_form_refuses_a_ladder_that_does_not_fit():
     betas = geometric_betas(64, 0.25, 5.0)
     with pytest.raises(_lib.EngineError, match="one cluster"):
