@@ -1212,6 +1212,49 @@ def call_latency(args):
     print(json.dumps(out), flush=True)
 
 
+def shape_table(args):
+    """Microseconds per sweep of the sparse engine on small problems for every round-end form
+    (grid, cluster) and item size (4 positions, 1 position), plus the automatic choice: the
+    measurements the automatic launch shape follows. 2e4 sweeps per entry after 200 warm-up
+    rounds, CUDA events, one GPU."""
+    import torch
+
+    from drift_b200.engine import DeviceProblem, HostProblem, PtEngine
+    from drift_b200.instances import ea_2d, gnp_pm
+
+    def us_per_sweep(model, R, spr, round_sync, ppi, sweeps=20000):
+        prob = DeviceProblem(HostProblem.from_model(model))
+        betas = 1.0 / np.geomspace(1 / 0.1, 1 / 3.0, R)
+        eng = PtEngine(prob, betas, seed=1, sweeps_per_round=spr, round_sync=round_sync, positions_per_item=ppi)
+        eng.init()
+        eng.run(200)
+        eng.check()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        eng.run(sweeps // spr)
+        e1.record()
+        e1.synchronize()
+        eng.check()
+        return e0.elapsed_time(e1) * 1e3 / sweeps
+
+    cases = [("2D EA L=16", lambda: ea_2d(16, 1), 24, 1), ("2D EA L=16", lambda: ea_2d(16, 1), 24, 4),
+             ("2D EA L=8", lambda: ea_2d(8, 1), 16, 1), ("G(400, 0.01) +-1", lambda: gnp_pm(400, 0.01, 3), 32, 1),
+             ("2D EA L=32", lambda: ea_2d(32, 1), 24, 1)]
+    rows = []
+    for name, make, R, spr in cases:
+        model = make()
+        row = {"problem": name, "R": R, "sweeps_per_round": spr}
+        for key, rs, ppi in (("grid_4", 1, 4), ("grid_1", 1, 1), ("cluster_4", 2, 4), ("cluster_1", 2, 1),
+                             ("auto", 0, 0)):
+            try:
+                row[key] = round(us_per_sweep(model, R, spr, rs, ppi), 3)
+            except Exception as e:  # a shape the device cannot hold
+                row[key] = f"unsupported: {str(e)[:60]}"
+        rows.append(row)
+    print(json.dumps({"metric": "microseconds per sweep", "unit": "us", "higher_is_better": False,
+                      "data": "synthetic", "rows": rows}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1237,9 +1280,13 @@ def main():
                     help="override the rounds per step (profiling of a short case; the line then says so)")
     ap.add_argument("--call-latency", action="store_true",
                     help="time one small solve()-style call: in-process drop-in vs the subprocess + file boundary")
+    ap.add_argument("--shape-table", action="store_true",
+                    help="sparse engine: us per sweep of small problems for each round-end form and item size")
     args = ap.parse_args()
     if args.call_latency:
         call_latency(args)
+    elif args.shape_table:
+        shape_table(args)
     elif args.impl == "reference":
         bench_reference(args)
     elif args.impl == "reference-gpu":
