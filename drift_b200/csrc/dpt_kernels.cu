@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelAr
       uint32_t* ent_sm = reinterpret_cast<uint32_t*>(smem + L.nbr);
       const int8_t* w8 = static_cast<const int8_t*>(a.ell_w);
       for (int i = tid; i < (int)a.n_ell; i += B)
-        ent_sm[i] = (uint32_t)a.ell_nbr[i] | ((uint32_t)(uint8_t)w8[i] << 24);
+        ent_sm[i] = ((uint32_t)a.ell_nbr[i] << 8) | (uint32_t)(uint8_t)w8[i];
     } else {
       const int4* s4 = reinterpret_cast<const int4*>(a.ell_nbr);
       int4* d4 = reinterpret_cast<int4*>(smem + L.nbr);

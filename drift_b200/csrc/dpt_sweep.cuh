@@ -52,11 +52,13 @@ __device__ __forceinline__ uint32_t range_mask(int p0, int lo, int hi) {
 }
 
 // Gather of the local fields of one item. W > 0 with kExactW: every slice has exactly W entries
-// per position, so all 2 * W * P shared loads are independent and issued before any use. W > 0
-// without kExactW: W bounds the width, loads beyond it are predicated off. W == 0: run-time loop.
+// per position (so slice S starts at entry block S * W), and all 2 * W * P shared loads are
+// independent and issued before any use. W > 0 without kExactW: W bounds the width, loads beyond it
+// are predicated off. W == 0: run-time loop. An integer-path entry is (neighbour position << 8) |
+// (uint8) weight: the spin's address is one shift-and-add of it.
 template <int W, bool kExactW, bool kInSmem, bool kField, int P>
 __device__ __forceinline__ void gather_int(int field[P], int S, int lane, int q0, uint32_t sp_o, const Tables& T) {
-  const int w0 = slice_off<kInSmem>(T, S);
+  const int w0 = kExactW ? S * W : slice_off<kInSmem>(T, S);
   const int width = kExactW ? W : slice_off<kInSmem>(T, S + 1) - w0;
   const uint32_t base = (uint32_t)w0 * kSlicePositions + lane;
 #pragma unroll
@@ -75,7 +77,7 @@ __device__ __forceinline__ void gather_int(int field[P], int S, int lane, int q0
         const uint32_t e = base + (uint32_t)d * kSlicePositions + (uint32_t)(q0 + i) * 32;
         if (kExactW || d < width) {
           if constexpr (kInSmem) ev[d][i] = lds_u32(T.ent_o + 4u * e);
-          else ev[d][i] = (uint32_t)__ldg(T.nbr + e) | ((uint32_t)(uint8_t)__ldg(T.w8 + e) << 24);
+          else ev[d][i] = ((uint32_t)__ldg(T.nbr + e) << 8) | (uint32_t)(uint8_t)__ldg(T.w8 + e);
         } else {
           ev[d][i] = 0u;  // neighbour 0 with weight 0
         }
@@ -84,11 +86,11 @@ __device__ __forceinline__ void gather_int(int field[P], int S, int lane, int q0
 #pragma unroll
     for (int d = 0; d < W; ++d)
 #pragma unroll
-      for (int i = 0; i < P; ++i) sv[d][i] = lds_s8(sp_o + (ev[d][i] & 0xFFFFFFu));
+      for (int i = 0; i < P; ++i) sv[d][i] = lds_s8(sp_o + (ev[d][i] >> 8));
 #pragma unroll
     for (int d = 0; d < W; ++d)
 #pragma unroll
-      for (int i = 0; i < P; ++i) field[i] += (((int)ev[d][i]) >> 24) * sv[d][i];
+      for (int i = 0; i < P; ++i) field[i] += (int)(int8_t)(uint8_t)ev[d][i] * sv[d][i];
   } else {
     for (int d = 0; d < width; ++d) {
       uint32_t ev[P];
@@ -96,10 +98,10 @@ __device__ __forceinline__ void gather_int(int field[P], int S, int lane, int q0
       for (int i = 0; i < P; ++i) {
         const uint32_t e = base + (uint32_t)d * kSlicePositions + (uint32_t)(q0 + i) * 32;
         if constexpr (kInSmem) ev[i] = lds_u32(T.ent_o + 4u * e);
-        else ev[i] = (uint32_t)__ldg(T.nbr + e) | ((uint32_t)(uint8_t)__ldg(T.w8 + e) << 24);
+        else ev[i] = ((uint32_t)__ldg(T.nbr + e) << 8) | (uint32_t)(uint8_t)__ldg(T.w8 + e);
       }
 #pragma unroll
-      for (int i = 0; i < P; ++i) field[i] += (((int)ev[i]) >> 24) * lds_s8(sp_o + (ev[i] & 0xFFFFFFu));
+      for (int i = 0; i < P; ++i) field[i] += (int)(int8_t)(uint8_t)ev[i] * lds_s8(sp_o + (ev[i] >> 8));
     }
   }
 }
@@ -157,7 +159,7 @@ __device__ __forceinline__ int group_int(int g, int b, int lo, int hi, uint32_t 
 
 template <int W, bool kExactW, bool kInSmem, bool kField>
 __device__ __forceinline__ void gather_f32(float field[kGroup], int S, int lane, uint32_t sp_o, const Tables& T) {
-  const int w0 = slice_off<kInSmem>(T, S);
+  const int w0 = kExactW ? S * W : slice_off<kInSmem>(T, S);
   const int width = kExactW ? W : slice_off<kInSmem>(T, S + 1) - w0;
   const uint32_t base = (uint32_t)w0 * kSlicePositions + lane;
 #pragma unroll
