@@ -202,10 +202,18 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelAr
     long long dacc = 0;
     const uint32_t thr_o = kInt ? (uint32_t)L.thr + 4u * (uint32_t)(rung_sm[my_slot] * (2 * a.F + 1) + a.F) : 0u;
     const float neg2beta = kInt ? 0.0f : nb_sm[active ? my_sl : 0];
+    // the class bounds never change during the launch: each phase reads the next phase's before
+    // its barrier, so no shared load starts the phase after it
+    int lo_n = cptr[0], hi_n = cptr[1];
     for (int sw = 0; sw < a.spr; ++sw) {
       const uint32_t t = (uint32_t)(round * a.spr + sw);
       for (int c = 0; c < k; ++c) {
-        const int lo = cptr[c], hi = cptr[c + 1];
+        const int lo = lo_n, hi = hi_n;
+        {
+          const int cn = c + 1 < k ? c + 1 : 0;
+          lo_n = cptr[cn];
+          hi_n = cptr[cn + 1];
+        }
         const int glo = lo >> 3, ghi = (hi + 7) >> 3;
         // item v -> (group, sub-block): 32 consecutive items are 32 consecutive groups (coalesced
         // coupling reads), the NB sub-blocks of those groups follow as the next 32-item runs
