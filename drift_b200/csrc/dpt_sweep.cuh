@@ -122,6 +122,10 @@ __device__ __forceinline__ int group_int(int g, int b, int lo, int hi, uint32_t 
   const uint32_t own_o = sp_o + (uint32_t)(g * kGroup + q0);
   uint64_t s8 = (uint64_t)*reinterpret_cast<const SW*>(dpt_smem + own_o);
   const uint32_t inmask = range_mask<P>(g * kGroup + q0, lo, hi);
+  // decisions of the item's positions as bit masks: accepted on the first 16 bits, and tied on
+  // them (then the second 16 bits decide); one branch per item for the rare ties, and the spin
+  // word updated once at the end
+  uint32_t flips = 0u, ties = 0u;
   int dacc = 0;
 #pragma unroll
   for (int i = 0; i < P; ++i) {
@@ -144,14 +148,34 @@ __device__ __forceinline__ int group_int(int g, int b, int lo, int hi, uint32_t 
     const uint32_t prim = (word >> sh) & 0xFFFFu;
     const uint32_t th = thr >> 16;
     const bool in = (inmask >> i) & 1u;
-    bool acc = (x <= 0) | (prim < th);
-    if (in & (x > 0) & (prim == th)) {  // the first 16 bits tie: draw the second half of this uniform
-      const U4 r2 = philox(U4{(uint32_t)(g * kGroup + q), t, slot, c_second}, k0, k1);
-      acc = (r2.x & 0xFFFFu) < (thr & 0xFFFFu);
-    }
-    acc = acc & in;
-    s8 ^= acc ? ((uint64_t)0xFEu << (8 * i)) : 0ull;  // +1 (0x01) <-> -1 (0xFF)
+    const bool acc = in & ((x <= 0) | (prim < th));
+    flips |= (uint32_t)acc << i;
+    ties |= (uint32_t)(in & (x > 0) & (prim == th)) << i;
     dacc += acc ? 2 * x : 0;
+  }
+  if (ties) {  // the first 16 bits tie: the second half of the uniform decides
+#pragma unroll
+    for (int i = 0; i < P; ++i)
+      if ((ties >> i) & 1u) {
+        const int x = (int)(int8_t)(uint8_t)(s8 >> (8 * i)) * field[i];
+        const uint32_t thr = lds_u32(thr_o + 4u * (uint32_t)x);
+        const U4 r2 = philox(U4{(uint32_t)(g * kGroup + q0 + i), t, slot, c_second}, k0, k1);
+        if ((r2.x & 0xFFFFu) < (thr & 0xFFFFu)) {
+          flips |= 1u << i;
+          dacc += 2 * x;
+        }
+      }
+  }
+  // bit i of 4 flip bits -> byte i: the four shifted copies (by 0, 7, 14, 21) do not overlap, so the
+  // product has no carries; then 0x01 <-> 0xFF (+1 <-> -1) in every flipped byte
+  if constexpr (P == 8) {
+    const uint32_t lo = ((flips & 15u) * 0x00204081u) & 0x01010101u;
+    const uint32_t hi = ((flips >> 4) * 0x00204081u) & 0x01010101u;
+    s8 ^= (((uint64_t)hi << 32) | lo) * 0xFEull;
+  } else if constexpr (P == 4) {
+    s8 ^= (uint64_t)(((flips * 0x00204081u) & 0x01010101u) * 0xFEu);
+  } else {
+    s8 ^= (uint64_t)(flips * 0xFEu);
   }
   *reinterpret_cast<SW*>(dpt_smem + own_o) = (SW)s8;
   return dacc;
