@@ -1,71 +1,102 @@
 """Ising models accepted by the engine.
 
-``IsingModel`` keeps the semantics of drift/ising.py:24-78 (dense J symmetrised as (J + J^T)/2 with
-a zero diagonal, E(s) = -1/2 s.J.s - h.s, dE_i = 2 s_i (J_i.s + h_i)), so a model built for the
-reference is accepted unchanged. ``SparseIsingModel`` holds the same energy as a CSR, for sizes
-where the reference's dense float64 J cannot exist (a 3-D L=64 lattice would need 550 GB).
+Energy convention (the interface of drift/ising.py:50-68, which every layer of the engine keeps):
+``E(s) = -1/2 s.J.s - h.s`` over a symmetric coupling matrix with a zero diagonal, and the energy
+change of flipping spin i is ``2 s_i (J_i.s + h_i)``. A dense matrix given by the caller is made
+symmetric by averaging it with its transpose (drift/ising.py:41), so an asymmetric input means what
+it means to the reference.
+
+Both model classes share one evaluator (`_IsingEnergy`) that works from coupling fields
+``F = J s`` computed for a whole batch of configurations at once: ``DenseIsingModel`` computes them
+with one matrix product, ``SparseIsingModel`` from its CSR without ever forming J (a 3-D L = 64
+lattice would need a 550 GB dense float64 matrix). Objects of the reference's own ``IsingModel``
+class are accepted unchanged wherever the engine takes a model (`model_csr` reads only ``.J``,
+``.h`` and ``.n``).
 """
 
 from __future__ import annotations
 
-from dataclasses import dataclass
-
 import numpy as np
 
 
-@dataclass
-class IsingModel:
-    """Dense classical Ising model; see drift/ising.py:24-78."""
+def _dense_csr(J: np.ndarray, n: int):
+    """(row_ptr, col_idx, weight f32) of the non-zero entries of a dense J in row-major order.
 
-    J: np.ndarray
+    Row-major order is the order drift/gpu.py:71-76 writes the CSR in; the greedy colouring visits
+    neighbours in this order, so keeping it keeps the reference's colouring.
+    """
+    nz = J != 0.0
+    row_ptr = np.zeros(n + 1, dtype=np.int32)
+    np.cumsum(nz.sum(axis=1), out=row_ptr[1:])
+    col_idx = np.nonzero(nz)[1].astype(np.int32)
+    return row_ptr, col_idx, J[nz].astype(np.float32)
+
+
+class _IsingEnergy:
+    """Energies of one or many configurations from the coupling fields ``J s`` of a subclass."""
+
     h: np.ndarray
-
-    def __post_init__(self) -> None:
-        self.J = np.asarray(self.J, dtype=np.float64)
-        self.h = np.asarray(self.h, dtype=np.float64)
-        if self.h.ndim != 1:
-            raise ValueError("h must be a 1-D field vector")
-        n = self.h.shape[0]
-        if self.J.shape != (n, n):
-            raise ValueError(f"J must be ({n}, {n}) to match h, got {self.J.shape}")
-        self.J = 0.5 * (self.J + self.J.T)
-        np.fill_diagonal(self.J, 0.0)
 
     @property
     def n(self) -> int:
-        return self.h.shape[0]
+        return int(self.h.shape[0])
 
-    def energy(self, s: np.ndarray) -> float:
-        s = np.asarray(s, dtype=np.float64)
-        return float(-0.5 * s @ self.J @ s - self.h @ s)
+    def coupling_fields(self, S: np.ndarray) -> np.ndarray:  # (m, n) -> (m, n): row k is J @ S[k]
+        raise NotImplementedError
 
     def energy_batch(self, S: np.ndarray) -> np.ndarray:
-        S = np.asarray(S, dtype=np.float64)
-        return -0.5 * np.einsum("mi,ij,mj->m", S, self.J, S, optimize=True) - S @ self.h
+        S = np.atleast_2d(np.asarray(S, dtype=np.float64))
+        return -np.sum(S * (0.5 * self.coupling_fields(S) + self.h), axis=1)
 
-    def delta_energy_flip(self, s: np.ndarray, i: int) -> float:
-        return float(2.0 * s[i] * (self.J[i] @ s + self.h[i]))
+    def energy(self, s: np.ndarray) -> float:
+        return float(self.energy_batch(s)[0])
 
     def local_fields(self, s: np.ndarray) -> np.ndarray:
-        return self.J @ s + self.h
+        return self.coupling_fields(np.atleast_2d(np.asarray(s, dtype=np.float64)))[0] + self.h
+
+    def delta_energy_flip(self, s: np.ndarray, i: int) -> float:
+        s = np.asarray(s, dtype=np.float64)
+        return float(2.0 * s[i] * self.local_fields(s)[i])
+
+
+class DenseIsingModel(_IsingEnergy):
+    """Ising model with a dense coupling matrix (float64), symmetrised with a zero diagonal."""
+
+    def __init__(self, J, h):
+        h = np.array(h, dtype=np.float64)
+        J = np.array(J, dtype=np.float64)
+        if h.ndim != 1:
+            raise ValueError(f"the field must be a vector, got an array of shape {h.shape}")
+        if J.shape != (h.size, h.size):
+            raise ValueError(f"couplings of shape {J.shape} do not match a field of {h.size} spins")
+        sym = J + J.T
+        sym *= 0.5
+        sym[np.diag_indices(h.size)] = 0.0
+        self.J = sym
+        self.h = h
+
+    def coupling_fields(self, S: np.ndarray) -> np.ndarray:
+        return S @ self.J  # J is symmetric
 
     @property
     def nbonds(self) -> int:
-        return int(np.count_nonzero(np.triu(self.J)))
+        """Undirected couplings (non-zero entries above the diagonal)."""
+        return int(np.count_nonzero(self.J)) // 2
 
     def csr(self):
-        """(row_ptr, col_idx, weight) of the non-zero couplings, as drift/gpu.py:71-76 builds them."""
-        rows, cols = np.nonzero(self.J)
-        weight = self.J[rows, cols].astype(np.float32)
-        row_ptr = np.zeros(self.n + 1, dtype=np.int32)
-        row_ptr[1:] = np.cumsum(np.bincount(rows, minlength=self.n))
-        return row_ptr, cols.astype(np.int32), weight
+        return _dense_csr(self.J, self.n)
 
 
-class SparseIsingModel:
-    """Ising model stored as a symmetric CSR (no dense J). Same energy convention as IsingModel.
+# The engine's own dense model under the domain's usual name (the reference's IsingModel objects
+# are accepted as they are; see `model_csr`).
+IsingModel = DenseIsingModel
 
-    Built from undirected edges (i, j, w) with i != j; duplicate edges are summed.
+
+class SparseIsingModel(_IsingEnergy):
+    """Ising model stored as a symmetric CSR (no dense J), same energy convention.
+
+    Built from undirected edges (i, j, w) with i != j; duplicate edges are summed and couplings that
+    sum to zero are dropped.
     """
 
     def __init__(self, n: int, edges_i, edges_j, weights, h=None):
@@ -109,40 +140,35 @@ class SparseIsingModel:
     def csr(self):
         return self._row_ptr.astype(np.int32), self._col, self._w.astype(np.float32)
 
-    def local_fields_nofield(self, s: np.ndarray) -> np.ndarray:
-        s = np.asarray(s, dtype=np.float64)
+    def coupling_fields(self, S: np.ndarray) -> np.ndarray:
+        # per row k: F[k, i] = sum over the CSR entries of row i of w * S[k, col]
         rows = np.repeat(np.arange(self._n), np.diff(self._row_ptr))
-        return np.bincount(rows, weights=self._w * s[self._col], minlength=self._n)
+        out = np.zeros((S.shape[0], self._n))
+        for k in range(S.shape[0]):
+            out[k] = np.bincount(rows, weights=self._w * S[k, self._col], minlength=self._n)
+        return out
 
-    def energy(self, s: np.ndarray) -> float:
-        s = np.asarray(s, dtype=np.float64)
-        return float(-0.5 * s @ self.local_fields_nofield(s) - self.h @ s)
-
-    def energy_batch(self, S: np.ndarray) -> np.ndarray:
-        return np.array([self.energy(s) for s in np.atleast_2d(S)])
+    def local_fields_nofield(self, s: np.ndarray) -> np.ndarray:
+        return self.coupling_fields(np.atleast_2d(np.asarray(s, dtype=np.float64)))[0]
 
     def delta_energy_flip(self, s: np.ndarray, i: int) -> float:
         a, b = self._row_ptr[i], self._row_ptr[i + 1]
-        return float(2.0 * s[i] * (self._w[a:b] @ np.asarray(s, dtype=np.float64)[self._col[a:b]] + self.h[i]))
+        s = np.asarray(s, dtype=np.float64)
+        return float(2.0 * s[i] * (self._w[a:b] @ s[self._col[a:b]] + self.h[i]))
 
-    def to_dense(self) -> IsingModel:
+    def to_dense(self) -> DenseIsingModel:
         J = np.zeros((self._n, self._n))
         rows = np.repeat(np.arange(self._n), np.diff(self._row_ptr))
         J[rows, self._col] = self._w
-        return IsingModel(J, self.h.copy())
+        return DenseIsingModel(J, self.h.copy())
 
 
 def model_csr(model):
     """(n, row_ptr, col_idx, weight f32, h f32) for any model with .csr() or a dense .J."""
     if hasattr(model, "csr"):
         row_ptr, col_idx, weight = model.csr()
-    else:  # a reference drift.ising.IsingModel (dense J): the CSR of drift/gpu.py:71-76
-        Jm = np.ascontiguousarray(model.J, dtype=np.float64)
-        rows, cols = np.nonzero(Jm)
-        weight = Jm[rows, cols].astype(np.float32)
-        row_ptr = np.zeros(model.n + 1, dtype=np.int32)
-        row_ptr[1:] = np.cumsum(np.bincount(rows, minlength=model.n))
-        col_idx = cols.astype(np.int32)
+    else:  # a reference drift.ising.IsingModel (dense J, already symmetric)
+        row_ptr, col_idx, weight = _dense_csr(np.asarray(model.J, dtype=np.float64), int(model.n))
     h = np.ascontiguousarray(model.h, dtype=np.float32)
     return int(model.n), np.ascontiguousarray(row_ptr, np.int32), np.ascontiguousarray(col_idx, np.int32), \
         np.ascontiguousarray(weight, np.float32), h

@@ -53,15 +53,21 @@ def build(force: bool = False) -> str:
 
 
 REF_BIN = os.path.join(HERE, "_ref", "ising_pt")
-REFERENCE_TREE = "/root/reference"
+
+
+def reference_tree() -> str | None:
+    """The reference (DRiFT) source tree named by the DRIFT_REFERENCE_TREE environment variable, if
+    it is set and holds the tree; None otherwise."""
+    root = os.environ.get("DRIFT_REFERENCE_TREE")
+    return root if root and os.path.isdir(os.path.join(root, "cuda")) else None
 
 
 def build_ref() -> str | None:
     """Compile the reference's own GPU engine (cuda/ising_pt.cu, unchanged) into _ref/ when its
-    source tree is present; returns the binary's path if it exists afterwards."""
-    src = os.path.join(REFERENCE_TREE, "cuda", "ising_pt.cu")
-    if os.path.exists(src):
-        r = subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE={REFERENCE_TREE}"], capture_output=True,
+    source tree is named by DRIFT_REFERENCE_TREE; returns the binary's path if it exists afterwards."""
+    root = reference_tree()
+    if root is not None and os.path.exists(os.path.join(root, "cuda", "ising_pt.cu")):
+        r = subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE={root}"], capture_output=True,
                            text=True)
         if r.returncode != 0:
             raise RuntimeError(f"reference GPU engine build failed:\n{r.stdout}\n{r.stderr}")

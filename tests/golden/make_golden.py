@@ -9,7 +9,12 @@ Needs the reference source tree on disk (it is imported, not copied). Writes:
   * ref_pt.json    - outputs of the reference CPU parallel tempering
     (drift/solvers/parallel_tempering.py:52-124) for fixed seeds: best_E, swap_rate, best_history;
   * bank_fixtures.json - the reference instance bank's n=8 fixtures (J, h, known energy) as
-    written by drift/benchmarks/instances/fixtures/*.json.
+    written by drift/benchmarks/instances/fixtures/*.json;
+  * solve_dispatch.json - what the reference dispatcher drift.solve.solve (drift/solve.py:75-80)
+    does on instances past its exact-enumeration size: the call it makes to
+    drift.gpu.parallel_tempering_gpu (positional model, keyword arguments), recorded by replacing
+    that function and drift.gpu.gpu_available, and how it turns the returned PtResult into its
+    Solution (method, certified flag, energy and configuration taken from best_E and best_s).
 The tests compare the oracle and the engine against these files; the reference is not needed to
 run the tests.
 """
@@ -106,8 +111,46 @@ def main(ref_root: str) -> None:
         bank.append({"id": d["id"], "n": d["n"], "edges": edges(J), "h": d["h"], "known_energy": d["known_energy"]})
     with open(os.path.join(OUT, "bank_fixtures.json"), "w") as f:
         json.dump(bank, f)
-    print(f"wrote {len(ref)} instances, {len(pt)} PT runs, {len(bank)} bank fixtures to {OUT}")
+    dispatch = solve_dispatch()
+    with open(os.path.join(OUT, "solve_dispatch.json"), "w") as f:
+        json.dump(dispatch, f)
+    print(f"wrote {len(ref)} instances, {len(pt)} PT runs, {len(bank)} bank fixtures, {len(dispatch)} solve() "
+          f"dispatches to {OUT}")
+
+
+def solve_dispatch():
+    """Record drift.solve.solve's GPU branch on MaxCut G(n, 0.3) instances, n = 20..30."""
+    import importlib
+
+    ref_gpu = importlib.import_module("drift.gpu")
+    ref_solve = importlib.import_module("drift.solve")  # the module (drift exports a function of that name)
+    from drift.builders.qubo import maxcut_ising, random_graph
+    from drift.solvers.parallel_tempering import PtResult
+
+    out = []
+    for n in (20, 24, 28, 30):
+        model = maxcut_ising(random_graph(n, p=0.3, seed=n))
+        calls = []
+        marker = np.where(np.arange(n) % 3 == 0, -1.0, 1.0)
+
+        def recorder(m, **kwargs):
+            calls.append({"n": int(m.n), "kwargs": kwargs})
+            return PtResult(best_s=marker.copy(), best_E=float(m.energy(marker)), temperatures=np.array([1.0]),
+                            swap_rate=0.5)
+
+        saved = ref_gpu.gpu_available, ref_gpu.parallel_tempering_gpu
+        ref_gpu.gpu_available, ref_gpu.parallel_tempering_gpu = (lambda: True), recorder
+        try:
+            sol = ref_solve.solve(model)
+        finally:
+            ref_gpu.gpu_available, ref_gpu.parallel_tempering_gpu = saved
+        assert len(calls) == 1
+        out.append({"n": n, "edges": edges(model.J), "h": model.h.tolist(), "call": calls[0],
+                    "method": sol.method, "certified": bool(sol.certified),
+                    "energy_is_best_E": bool(sol.energy == float(model.energy(marker))),
+                    "s_is_best_s": bool(np.array_equal(sol.s, marker))})
+    return out
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DRIFT_REFERENCE", "."))
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DRIFT_REFERENCE_TREE", "."))

@@ -41,9 +41,9 @@ def test_result_fields_extend_the_reference_record():
 
 
 def _reference():
-    root = os.environ.get("DRIFT_REFERENCE_TREE", "/root/reference")
-    if not os.path.isdir(os.path.join(root, "drift")):
-        pytest.skip("reference tree not present")
+    root = os.environ.get("DRIFT_REFERENCE_TREE")
+    if not root or not os.path.isdir(os.path.join(root, "drift")):
+        pytest.skip("DRIFT_REFERENCE_TREE does not name the reference tree")
     sys.dont_write_bytecode = True
     if root not in sys.path:
         sys.path.append(root)

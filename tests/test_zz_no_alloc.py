@@ -5,7 +5,10 @@ cudaMalloc after start-up, a binding that only gets pointers to other people's b
 provide drift_pt_run's workspace. The allocation-free entry point uses the library's built-in
 scratch array instead; apart from that it must run the very same chain. This test calls it through
 the C ABI twice in a row (a fresh chain, then a resumed one) and compares every output with the
-workspace entry point's, bit for bit as the other parity tests do. It also checks the size limit.
+workspace entry point's, bit for bit as the other parity tests do, checking after each call with
+drift_pt_noalloc_check that no bounded wait gave up. It also checks the size limit at its exact
+boundary (the largest replica count, whose scratch fills the array) and one past it, and that a run
+whose wait limit runs out is reported by drift_pt_noalloc_check and leaves the next run clean.
 
 The file is named to be collected last, so a run that stops at the first failure has run every
 other test before this one; it does not depend on them and passes alone in a fresh process.
@@ -23,15 +26,22 @@ from conftest import cuda_ready
 from drift_b200 import _lib
 from drift_b200.engine import DeviceProblem, HostProblem, PtEngine, geometric_betas
 from drift_b200.instances import maxcut_3regular
+from drift_b200.ising import IsingModel
 
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not cuda_ready(), reason="needs CUDA and libdrift_pt.so")]
 
 
-def _run_noalloc(eng: PtEngine, n_rounds: int, hist) -> None:
+def _run_noalloc(eng: PtEngine, n_rounds: int, hist=None, timeout_s: float | None = None) -> None:
     L = _lib.load()
     P, A, S = eng.prob.c_problem(), eng._args(n_rounds), eng._state(hist)
+    if timeout_s is not None:
+        A.timeout_s = timeout_s
     _lib.check(L.drift_pt_run_noalloc(C.byref(P), C.byref(A), C.byref(S), eng.stream()), "drift_pt_run_noalloc")
     eng.rounds_done += n_rounds
+
+
+def _noalloc_check(eng: PtEngine) -> int:
+    return _lib.load().drift_pt_noalloc_check(eng.stream())
 
 
 def test_noalloc_entry_matches_workspace_entry_on_two_calls():
@@ -52,6 +62,7 @@ def test_noalloc_entry_matches_workspace_entry_on_two_calls():
         ref.run(n_rounds, history=h_ref)
         _run_noalloc(nal, n_rounds, h_nal)
         ref.check()
+        assert _noalloc_check(nal) == _lib.OK, f"call {call}: a bounded wait gave up"
         torch.cuda.synchronize()
         a, b = ref.fetch(), nal.fetch()
         for key in ("spins", "best_spins", "energy_fixed", "best_energy_fixed", "rung_of_slot", "slot_of_rung",
@@ -72,3 +83,56 @@ def test_noalloc_entry_rejects_too_many_replicas():
     rc = L.drift_pt_run_noalloc(C.byref(prob.c_problem()), C.byref(args), C.byref(eng._state()), eng.stream())
     assert rc == _lib.EUNSUPPORTED
     assert "4096" in L.drift_pt_last_error().decode()
+
+
+def test_noalloc_entry_at_its_replica_limit():
+    """R = DRIFT_PT_NOALLOC_MAX_REPLICAS: the scratch the run needs is exactly the built-in array."""
+    import torch
+
+    R = 4096
+    need = C.c_size_t(0)
+    L = _lib.load()
+    _lib.check(L.drift_pt_workspace_bytes(R, C.byref(need)), "drift_pt_workspace_bytes")
+    assert need.value == 256 + 32 * R  # the array's size
+    # 4096 replicas fit the sweep kernel's shared memory when the largest local field is 1: 16 spins
+    # with fields of +-1 and no couplings
+    h = np.random.default_rng(3).choice([-1.0, 1.0], size=16)
+    model = IsingModel(np.zeros((16, 16)), h)
+    prob = DeviceProblem(HostProblem.from_model(model))
+    assert prob.integer_path and prob.max_field == 1
+    betas = geometric_betas(R, 0.2, 4.0)
+    ref = PtEngine(prob, betas, seed=3, sweeps_per_round=1)
+    nal = PtEngine(prob, betas, seed=3, sweeps_per_round=1)
+    ref.init()
+    nal.init()
+    h_ref = torch.zeros(1, dtype=torch.float64, device=prob.device)
+    h_nal = torch.zeros(1, dtype=torch.float64, device=prob.device)
+    ref.run(1, history=h_ref)
+    _run_noalloc(nal, 1, h_nal)
+    ref.check()
+    assert _noalloc_check(nal) == _lib.OK
+    a, b = ref.fetch(), nal.fetch()
+    for key in ("spins", "best_spins", "energy_fixed", "best_energy_fixed", "rung_of_slot", "slot_of_rung",
+                "tried", "accepted"):
+        assert np.array_equal(a[key], b[key]), key
+    assert torch.equal(h_ref, h_nal)
+
+
+def test_noalloc_check_reports_a_wait_that_ran_out():
+    """A wait limit of 1 ns runs out at the first grid-wide wait; the kernel gives up (it sets the
+    error flag, every CTA leaves its round loop) and the check reports it. The next call with the
+    default limit starts from a cleared scratch and is clean."""
+    model = maxcut_3regular(1024, 4)
+    prob = DeviceProblem(HostProblem.from_model(model))
+    betas = geometric_betas(32, 0.25, 5.0)
+    eng = PtEngine(prob, betas, seed=9, sweeps_per_round=1, replicas_per_cta=1, round_sync=1)
+    eng.init()
+    _run_noalloc(eng, 200, timeout_s=1e-9)
+    rc = _noalloc_check(eng)
+    assert rc == _lib.ETIMEOUT, rc
+    assert "timed out" in _lib.load().drift_pt_last_error().decode()
+    eng.init()
+    _run_noalloc(eng, 3)
+    assert _noalloc_check(eng) == _lib.OK
+    st = eng.fetch()
+    assert np.array_equal(eng.energy_fp64(), st["energy_fixed"].astype(np.float64))
