@@ -221,26 +221,53 @@ def barrier(world: int):
 
 # ---------------------------------------------------------------------------------------------
 
+# seconds of host work per CPU baseline (the secondaries use less)
+CPU_BUDGET_S = 12.0
+
+
+def emit(args, line: dict) -> None:
+    """Print a result line, or hand it to the caller that runs this workload as a secondary."""
+    sink = getattr(args, "sink", None)
+    if sink is not None:
+        sink.append(line)
+    else:
+        print(json.dumps(line), flush=True)
+
+
 REF_SAMPLE_RUNGS = 64
+# attempts per process and step of the reference arm's sample (about 2-5 s of one core)
+REF_SAMPLE_ATTEMPTS = 1.0e6
+_REF_WORKER = {}
+
+
+def _ref_worker_init(name):
+    """Pool initializer: the reference's dense model of the workload, built once per process."""
+    sys.path.insert(0, ROOT)
+    model = make_model(name)
+    _REF_WORKER["model"] = model.to_dense() if hasattr(model, "to_dense") else model
+
+
+def ref_sample_shape(w, n):
+    """(rungs, rounds) of one process's sample: the reference's cost is linear in rungs, so wide
+    ladders are sampled with REF_SAMPLE_RUNGS rungs over the same temperature range, and rounds are
+    added up to about REF_SAMPLE_ATTEMPTS attempts."""
+    rungs = min(w["R"], REF_SAMPLE_RUNGS)
+    return rungs, max(1, int(round(REF_SAMPLE_ATTEMPTS / (rungs * w["spr"] * n))))
 
 
 def run_reference_sample(args_tuple):
-    """One process: the reference CPU algorithm on a bounded sample (1 round x 1 sweep of all rungs)."""
+    """One process: the reference CPU algorithm on a bounded sample; returns (attempts, seconds of
+    the round loop alone)."""
     name, seed = args_tuple
-    os.environ["OMP_NUM_THREADS"] = "1"
-    sys.path.insert(0, ROOT)
     from oracle import ref_pt
 
     w = WORKLOADS[name]
-    model = make_model(name)
-    model = model.to_dense() if hasattr(model, "to_dense") else model
+    model = _REF_WORKER["model"]
     b = ladder(w)
-    t0 = time.perf_counter()
-    # the reference's cost is linear in rungs: wide ladders are sampled with REF_SAMPLE_RUNGS rungs over the
-    # same temperature range
-    out = ref_pt.parallel_tempering(model, n_replicas=min(w["R"], REF_SAMPLE_RUNGS), T_min=1.0 / b[0],
-                                    T_max=1.0 / b[-1], n_rounds=1, sweeps_per_round=1, seed=seed)
-    return out["attempts"], time.perf_counter() - t0
+    rungs, rounds = ref_sample_shape(w, model.n)
+    out = ref_pt.parallel_tempering(model, n_replicas=rungs, T_min=1.0 / b[0], T_max=1.0 / b[-1], n_rounds=rounds,
+                                    sweeps_per_round=w["spr"], seed=seed)
+    return out["attempts"], out["loop_seconds"]
 
 
 def bench_reference(args):
@@ -256,28 +283,32 @@ def bench_reference(args):
 
     w = WORKLOADS[args.workload]
     n_sample = make_model(args.workload).n
+    rungs, rounds = ref_sample_shape(w, n_sample)
     where = " of the batch's median-size instance" if "n_instances" in w else ""
     cores = os.cpu_count() or 1
+    # one BLAS thread per process: the workers are spawned with this environment
+    for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[var] = "1"
     ctx = mp.get_context("spawn")
-    with ctx.Pool(cores) as pool:
+    with ctx.Pool(cores, initializer=_ref_worker_init, initargs=(args.workload,)) as pool:
         for s in range(args.warmup):
             pool.map(run_reference_sample, [(args.workload, 1000 * s + c) for c in range(cores)])
-        t0 = time.perf_counter()
-        total = 0.0
+        total, t_sum = 0.0, 0.0
         for s in range(args.steps):
             res = pool.map(run_reference_sample, [(args.workload, 1000 * (s + args.warmup) + c) for c in range(cores)])
             total += sum(a for a, _ in res)
-        wall = time.perf_counter() - t0
-    v = total / wall / 1e9
+            t_sum += max(t for _, t in res)  # the processes run side by side: the step lasts as long as the slowest
+    v = total / t_sum / 1e9
+    sample = (f"{cores} processes x ({rounds} rounds x {w['spr']} sweeps x {rungs} rungs x {n_sample} spins{where}) "
+              f"per step; each process's round loop timed (dense model built once per process, initial energies "
+              f"excluded), the slowest process per step")
     print(json.dumps({
         "impl": "reference", "metric": "spin-flips/ns", "value": v, "unit": "flips/ns", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_sum / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": w["desc"], "sample": f"{cores} processes x (1 round x 1 sweep x "
-                   f"{min(w['R'], REF_SAMPLE_RUNGS)} rungs x {n_sample} spins{where}) per step"},
+        "config": {"workload": w["desc"], "sample": sample},
         "cpu_baseline": {"value": v, "unit": "flips/ns", "cores": cores, "kind": "port",
-                         "sample": f"oracle/ref_pt.py (reference CPU PT restated, same NumPy stream), one process per core, "
-                                   f"{cores} x {min(w['R'], REF_SAMPLE_RUNGS) * n_sample:.0f} attempts per step"},
+                         "sample": "oracle/ref_pt.py (the reference CPU PT restated, same NumPy stream): " + sample},
         "e2e": {"value": v, "unit": "flips/ns", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -297,7 +328,7 @@ def bench_reference_gpu(args):
     if not os.path.exists(oracle.REF_BIN) or args.workload not in ("maxcut3reg", "ea2d", "sk512"):
         why = "oracle/_ref/ising_pt not built" if not os.path.exists(oracle.REF_BIN) else \
             "the reference engine runs one instance of a CSR model (no batched or bit-packed input)"
-        print(json.dumps({"impl": "reference-gpu", "unavailable": why}), flush=True)
+        emit(args, {"impl": "reference-gpu", "unavailable": why})
         return
     model = make_model(args.workload)
     b = ladder(w)
@@ -313,14 +344,14 @@ def bench_reference_gpu(args):
             r = subprocess.run([oracle.REF_BIN, prob, res], capture_output=True, text=True, timeout=1800)
             wall = time.perf_counter() - t0
             if r.returncode != 0:
-                print(json.dumps({"impl": "reference-gpu", "unavailable": f"reference engine failed: {r.stderr[-300:]}"}))
+                emit(args, {"impl": "reference-gpu", "unavailable": f"reference engine failed: {r.stderr[-300:]}"})
                 return
             if s_ >= args.warmup:
                 f = parse_stderr(r.stderr)
                 vals.append(f["throughput"] / 1e9)
                 walls.append(float(w["R"]) * rounds * w["spr"] * w["n"] / wall / 1e9)
                 bests.append(read_result(res, w["n"])[0])
-    print(json.dumps({
+    emit(args, {
         "impl": "reference-gpu", "metric": "spin-flips/ns", "value": float(np.median(vals)), "unit": "flips/ns",
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64 field, f32 spins",
         "data": "synthetic",
@@ -328,11 +359,12 @@ def bench_reference_gpu(args):
                    "timer": "the reference's own (round loop, device-synchronised)"},
         "wall_clock_flips_per_ns": float(np.median(walls)), "best_energy": float(np.min(bests)),
         "binary": "oracle/_ref/ising_pt: cuda/ising_pt.cu compiled unchanged with -gencode arch=compute_100a,code=sm_100a",
-    }), flush=True)
+    })
 
 
-def cpu_baseline_oracle(w, model_name, budget_s=12.0):
+def cpu_baseline_oracle(w, model_name, budget_s=None):
     """The C oracle (OpenMP over replicas) on the host cores: a bounded number of rounds."""
+    budget_s = CPU_BUDGET_S if budget_s is None else budget_s
     import oracle
 
     from drift_b200.engine import HostProblem
@@ -374,7 +406,8 @@ def bench_b200(args):
     prob = DeviceProblem(hp, device=dev)
     betas = ladder(w)
     rounds = args.rounds or w["sweeps"] // w["spr"]
-    eng = PtEngine(prob, betas, seed=1, sweeps_per_round=w["spr"], instance=rank)
+    eng = PtEngine(prob, betas, seed=1, sweeps_per_round=w["spr"], instance=rank, item_form=args.item_form,
+                   positions_per_item=args.positions_per_item)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     attempts_per_step = float(w["R"]) * rounds * w["spr"] * w["n"]
 
@@ -446,7 +479,8 @@ def bench_b200(args):
                        "rounds": rounds, "sweeps_per_round": w["spr"],
                        "attempts_per_step": attempts_per_step, "parallelism": f"replicas-only x{world}",
                        "l2": "flushed between steps (256 MiB write)",
-                       "launch": {"rpc": eng.rpc or "auto", "threads": eng.threads or "auto"}},
+                       "launch": {"rpc": eng.rpc or "auto", "threads": eng.threads or "auto",
+                                  "item_form": {0: "auto", 1: "gather", 2: "unit-regular"}[args.item_form]}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "pt_run_kernel", "bytes_per_attempt": w["bytes_per_attempt"],
@@ -458,11 +492,59 @@ def bench_b200(args):
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_oracle(w, args.workload)
-        print(json.dumps(line), flush=True)
+        if world == 1 and args.workload == "maxcut3reg" and not args.no_secondary and not args.rounds:
+            line["secondary"] = secondaries(args)
+        emit(args, line)
     if world > 1:
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+# The other BASELINE workloads measured alongside the default line: (key, workload, overrides).
+SECONDARIES = [
+    ("ea2d_C1", "ea2d", {}),
+    ("batched_er_C3", "batched_er", {}),
+    ("sk512_C4", "sk512", {"ttt": True, "ttt_seeds": 3}),
+    ("ea3d64_C5", "ea3d64", {}),
+    ("ea2d_batch256_C5b", "ea2d_batch256", {}),
+    ("maxcut3reg_r2048", "maxcut3reg_r2048", {}),
+]
+# the reference's own GPU engine (cuda/ising_pt.cu built unchanged into oracle/_ref) on shortened jobs
+REFERENCE_GPU = [("maxcut3reg_C2", "maxcut3reg", 2500), ("ea2d_C1", "ea2d", 20000)]
+
+
+def secondaries(args) -> dict:
+    """Run the other workloads with 3 warm-up and 3 timed steps each and collect their lines; then the
+    reference GPU engine on C2 and C1. Each entry is that workload's own line (or an error)."""
+    import copy
+
+    global CPU_BUDGET_S
+    saved_budget, CPU_BUDGET_S = CPU_BUDGET_S, 4.0
+    out = {}
+    for key, workload, over in SECONDARIES:
+        a = copy.copy(args)
+        a.workload, a.steps, a.warmup, a.rounds, a.sink = workload, 3, 3, 0, []
+        a.item_form, a.positions_per_item, a.ttt = 0, 0, False
+        for k, v in over.items():
+            setattr(a, k, v)
+        try:
+            t0 = time.perf_counter()
+            run_workload(a)
+            out[key] = a.sink[-1] if a.sink else {"error": "no line"}
+            out[key]["wall_s"] = time.perf_counter() - t0
+        except Exception as e:  # noqa: BLE001 - a failing secondary must not lose the headline
+            out[key] = {"error": f"{type(e).__name__}: {e}"[:300]}
+    for key, workload, rounds in REFERENCE_GPU:
+        a = copy.copy(args)
+        a.workload, a.steps, a.warmup, a.rounds, a.sink = workload, 1, 1, rounds, []
+        try:
+            bench_reference_gpu(a)
+            out["reference_gpu_" + key] = a.sink[-1] if a.sink else {"error": "no line"}
+        except Exception as e:  # noqa: BLE001
+            out["reference_gpu_" + key] = {"error": f"{type(e).__name__}: {e}"[:300]}
+    CPU_BUDGET_S = saved_budget
+    return out
 
 
 def load_tensor_peak():
@@ -474,8 +556,9 @@ def load_tensor_peak():
     return 1400.0, "fallback (bf16 sustained)"
 
 
-def cpu_baseline_sk(w, sk, budget_s=12.0):
+def cpu_baseline_sk(w, sk, budget_s=None):
     """The C oracle of the dense chain (OpenMP over replicas) on the host cores, bounded."""
+    budget_s = CPU_BUDGET_S if budget_s is None else budget_s
     import oracle
 
     b = ladder(w)
@@ -590,15 +673,16 @@ def bench_sk(args):
             line["cpu_baseline"] = cpu_baseline_sk(w, sk)
         if args.ttt:
             line["time_to_target"] = time_to_target(w, sk, args, dev)
-        print(json.dumps(line), flush=True)
+        emit(args, line)
     if world > 1:
         import torch.distributed as dist
 
         dist.destroy_process_group()
 
 
-def cpu_baseline_ms(w, lat, budget_s=12.0):
+def cpu_baseline_ms(w, lat, budget_s=None):
     """The multispin oracle (one replica bit at a time) on a bounded number of sweeps."""
+    budget_s = CPU_BUDGET_S if budget_s is None else budget_s
     import oracle
 
     b = ladder(w)
@@ -701,15 +785,16 @@ def bench_ms(args):
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_ms(w, lat)
-        print(json.dumps(line), flush=True)
+        emit(args, line)
     if world > 1:
         import torch.distributed as dist
 
         dist.destroy_process_group()
 
 
-def cpu_baseline_gms(w, lay, budget_s=12.0):
+def cpu_baseline_gms(w, lay, budget_s=None):
     """The graph multispin oracle (scalar, one replica bit at a time) on a bounded number of rounds."""
+    budget_s = CPU_BUDGET_S if budget_s is None else budget_s
     import oracle
 
     b = ladder(w)
@@ -818,7 +903,7 @@ def bench_gms(args):
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_gms(w, lay)
-        print(json.dumps(line), flush=True)
+        emit(args, line)
     if world > 1:
         import torch.distributed as dist
 
@@ -860,8 +945,9 @@ def time_to_target(w, sk, args, dev):
             sweeps += chunk * spr
         dt = time.perf_counter() - t0
         out["plain"].append({"seed": seed, "seconds": dt, "sweeps": sweeps, "reached": reached(eng)})
-        # neural: the same start; plain rounds that collect the training set, training, then rounds
-        # with proposals at the 8 coldest rungs
+        # neural: the same start. Plain rounds collect the training set from the 8 coldest rungs;
+        # the network then trains on a second stream while plain PT goes on in the first (the dense
+        # kernel holds 32 of the 148 SMs), and proposals start when training is done
         eng = SkEngine(sk, betas, seed=seed, sweeps_per_round=spr, replicas_per_cta=args.sk_g, device=dev)
         eng.init()
         torch.cuda.synchronize()
@@ -869,9 +955,22 @@ def time_to_target(w, sk, args, dev):
         data = collect_cold_samples(eng, args.ttt_samples, n_cold=8)
         t_collect = time.perf_counter() - t0
         made = Made(w["n"], (1024, 1024), seed=seed, device=dev)
-        made.train(data, epochs=args.ttt_epochs, batch=512, lr=1e-3)
+        main, side = torch.cuda.current_stream(), torch.cuda.Stream(device=dev)
+        side.wait_stream(main)
+        steps_done, slice_steps = 0, 8
+        while steps_done < args.ttt_train_steps and not reached(eng) and time.perf_counter() - t0 < args.ttt_cap_s:
+            eng.run(chunk // 10)
+            with torch.cuda.stream(side):
+                k = min(slice_steps, args.ttt_train_steps - steps_done)
+                made.train_async(data, steps=k, batch=args.ttt_batch_size, lr=args.ttt_lr, seed=1000 * seed + steps_done)
+            steps_done += k
+        trained = torch.cuda.Event()
+        trained.record(side)
+        while not trained.query() and not reached(eng) and time.perf_counter() - t0 < args.ttt_cap_s:
+            eng.run(chunk // 10)
+        main.wait_stream(side)
         t_train = time.perf_counter() - t0 - t_collect
-        npt = NeuralPT(sk, betas, made, n_cold=8, engine=eng)
+        npt = NeuralPT(sk, betas, made, n_cold=8, engine=eng, suffix=args.ttt_suffix or None)
         rounds = 0
         while not reached(eng) and time.perf_counter() - t0 < args.ttt_cap_s:
             npt.run(chunk // 10)
@@ -879,8 +978,22 @@ def time_to_target(w, sk, args, dev):
         dt = time.perf_counter() - t0
         acc = npt.acceptance()[-8:]
         out["neural"].append({"seed": seed, "seconds": dt, "reached": reached(eng), "collect_s": t_collect,
-                              "train_s": t_train, "proposal_rounds": rounds,
+                              "train_s_overlapped_with_plain_pt": t_train, "train_steps": steps_done,
+                              "proposal_rounds": rounds,
                               "proposal_acceptance_cold8": float(np.nanmean(acc)) if np.isfinite(acc).any() else None})
+        if seed == 1:
+            # acceptance at the 8 coldest rungs against the number of spins a proposal redraws (the last m
+            # in the network's order; m = n is an independent whole configuration), from the state reached
+            sweep_acc = {}
+            for m in (4, 8, 16, 32, 64, 128, w["n"]):
+                probe = NeuralPT(sk, betas, made, n_cold=8, engine=eng, suffix=None if m == w["n"] else m)
+                t1 = time.perf_counter()
+                probe.run(40)
+                torch.cuda.synchronize()
+                a8 = probe.acceptance()[-8:]
+                sweep_acc[str(m)] = {"acceptance_cold8": float(np.nanmean(a8)) if np.isfinite(a8).any() else None,
+                                     "ms_per_round": (time.perf_counter() - t1) / 40 * 1e3}
+            out["acceptance_vs_redrawn_spins"] = sweep_acc
     for k in ("plain", "neural"):
         ts = [r["seconds"] for r in out[k]]
         out[k + "_median_s"] = float(np.median(ts))
@@ -910,19 +1023,12 @@ def bench_batched(args):
     shape = autotune(eng, rounds=2)
     total_n = int(sum(int(d["n"]) for d in bp.desc))
     attempts_per_step = float(w["R"]) * total_n * rounds * w["spr"]
-    # the timed step is a replay of a captured CUDA graph of the step's rounds (10 launches)
-    eng.run(1)
-    torch.cuda.synchronize()
-    chunk = max(1, rounds // 10)
-    g = torch.cuda.CUDAGraph()
-    with torch.cuda.graph(g):
-        done = 0
-        while done < rounds:
-            c = min(chunk, rounds - done)
-            eng.run(c)
-            done += c
+    # the timed step is one replay of a job captured whole as a CUDA graph (BatchEngine.capture_job:
+    # initialisation and the step's rounds, in 10 launches)
+    job = eng.capture_job(rounds, max(1, rounds // 10))
+    g = job.graph
     for _ in range(args.warmup):
-        g.replay()
+        job.replay()
     eng.check()
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     sampler = ClockSampler(local)
@@ -972,10 +1078,11 @@ def bench_batched(args):
             "e2e": {"value": attempts_per_step * world / t_e2e / 1e9, "unit": "flips/ns", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": int(bp2.total_slots * 8), "api": "BatchProblem + BatchEngine (Python)",
                     "best_energy_mean": float(np.mean(best))},
-            "gpu_launches": 10 * args.steps,
+            # per replay: the job's sweep launches and drift_pt_batch_init's three kernels per instance
+            "gpu_launches": (job.launches + 3 * bp.n_instances) * args.steps,
             "clocks": clocks,
         }
-        print(json.dumps(line), flush=True)
+        emit(args, line)
     if world > 1:
         import torch.distributed as dist
 
@@ -1152,107 +1259,11 @@ def bench_ea2d_batch(args):
         }
         if args.ttt and world == 1:
             line["time_to_target"] = ttt_batch(w, bp, hps, args, dev)
-        print(json.dumps(line), flush=True)
+        emit(args, line)
     if world > 1:
         import torch.distributed as dist
 
         dist.destroy_process_group()
-
-
-def call_latency(args):
-    """Wall time of one small solve()-style call (the reference's default PT settings: 16 replicas,
-    T 0.1-5, 300 rounds x 5 sweeps) on 20- and 40-spin +-1 instances, three ways: the in-process
-    drop-in parallel_tempering_gpu, the reference's own GPU engine behind its subprocess + problem
-    file boundary (drift/gpu.py:83-114; the binary built from cuda/ising_pt.cu into oracle/_ref),
-    and this engine's ising_pt command behind the same boundary. Median over `steps` calls after
-    `warmup`; the subprocess rows include process start and CUDA context creation, as the
-    reference's path does on every call."""
-    import tempfile
-
-    import torch
-
-    import oracle
-    from drift_b200.build import CLI_PATH
-    from drift_b200.gpu import parallel_tempering_gpu
-    from drift_b200.instances import gnp_pm
-    from drift_b200.problem_io import read_result, write_problem
-
-    torch.cuda.init()
-    kw = dict(n_replicas=16, T_min=0.1, T_max=5.0, n_rounds=300, sweeps_per_round=5)
-    out = {"metric": "seconds per solve() call", "unit": "s", "higher_is_better": False, "data": "synthetic",
-           "config": {"workload": "G(n, p) +-1 instances, n = 20 and 40; 16 replicas, T 0.1-5, 300 rounds x 5 sweeps",
-                      "steps": args.steps, "warmup": args.warmup, "statistic": "median"}, "rows": []}
-
-    def median_time(fn):
-        for _ in range(args.warmup):
-            fn()
-        ts = []
-        for _ in range(args.steps):
-            t0 = time.perf_counter()
-            fn()
-            ts.append(time.perf_counter() - t0)
-        return float(np.median(ts))
-
-    with tempfile.TemporaryDirectory() as d:
-        prob, res = os.path.join(d, "problem.bin"), os.path.join(d, "result.bin")
-        for n, pp in ((20, 0.3), (40, 0.15)):
-            model = gnp_pm(n, pp, 7)
-            row = {"n": n, "drop_in_s": median_time(lambda: parallel_tempering_gpu(model, seed=1, **kw))}
-
-            def through_files(binary):
-                write_problem(prob, model, seed=1, **kw)
-                r = subprocess.run([binary, prob, res], capture_output=True, text=True)
-                if r.returncode != 0:
-                    raise RuntimeError(r.stderr[-300:])
-                read_result(res, n)
-
-            for key, binary in (("reference_subprocess_s", oracle.REF_BIN), ("ising_pt_command_s", CLI_PATH)):
-                row[key] = median_time(lambda: through_files(binary)) if os.path.exists(binary) else None
-            out["rows"].append(row)
-    print(json.dumps(out), flush=True)
-
-
-def shape_table(args):
-    """Microseconds per sweep of the sparse engine on small problems for every round-end form
-    (grid, cluster) and item size (4 positions, 1 position), plus the automatic choice: the
-    measurements the automatic launch shape follows. 2e4 sweeps per entry after 200 warm-up
-    rounds, CUDA events, one GPU."""
-    import torch
-
-    from drift_b200.engine import DeviceProblem, HostProblem, PtEngine
-    from drift_b200.instances import ea_2d, gnp_pm
-
-    def us_per_sweep(model, R, spr, round_sync, ppi, sweeps=20000):
-        prob = DeviceProblem(HostProblem.from_model(model))
-        betas = 1.0 / np.geomspace(1 / 0.1, 1 / 3.0, R)
-        eng = PtEngine(prob, betas, seed=1, sweeps_per_round=spr, round_sync=round_sync, positions_per_item=ppi)
-        eng.init()
-        eng.run(200)
-        eng.check()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        eng.run(sweeps // spr)
-        e1.record()
-        e1.synchronize()
-        eng.check()
-        return e0.elapsed_time(e1) * 1e3 / sweeps
-
-    cases = [("2D EA L=16", lambda: ea_2d(16, 1), 24, 1), ("2D EA L=16", lambda: ea_2d(16, 1), 24, 4),
-             ("2D EA L=8", lambda: ea_2d(8, 1), 16, 1), ("G(400, 0.01) +-1", lambda: gnp_pm(400, 0.01, 3), 32, 1),
-             ("2D EA L=32", lambda: ea_2d(32, 1), 24, 1)]
-    rows = []
-    for name, make, R, spr in cases:
-        model = make()
-        row = {"problem": name, "R": R, "sweeps_per_round": spr}
-        for key, rs, ppi in (("grid_4", 1, 4), ("grid_1", 1, 1), ("cluster_4", 2, 4), ("cluster_1", 2, 1),
-                             ("auto", 0, 0)):
-            try:
-                row[key] = round(us_per_sweep(model, R, spr, rs, ppi), 3)
-            except Exception as e:  # a shape the device cannot hold
-                row[key] = f"unsupported: {str(e)[:60]}"
-        rows.append(row)
-    print(json.dumps({"metric": "microseconds per sweep", "unit": "us", "higher_is_better": False,
-                      "data": "synthetic", "rows": rows}), flush=True)
 
 
 def main():
@@ -1268,30 +1279,36 @@ def main():
     ap.add_argument("--ttt-seeds", type=int, default=3)
     ap.add_argument("--ttt-cap-s", type=float, default=20.0)
     ap.add_argument("--ttt-ref-sweeps", type=int, default=100000)
-    ap.add_argument("--ttt-samples", type=int, default=100000)
+    ap.add_argument("--ttt-samples", type=int, default=8192, help="neural PT (dense): training configurations")
     ap.add_argument("--ttt-epochs", type=int, default=5)
     ap.add_argument("--ttt-lr", type=float, default=1e-3, help="neural PT: Adam learning rate")
     ap.add_argument("--ttt-batch-size", type=int, default=512, help="neural PT: training batch")
+    ap.add_argument("--ttt-train-steps", type=int, default=600, help="neural PT (dense): Adam steps")
+    ap.add_argument("--ttt-suffix", type=int, default=0,
+                    help="neural PT (dense): redraw the last m spins per proposal (0 = whole configurations)")
     ap.add_argument("--ttt-propose-every", type=int, default=1,
                     help="batched neural PT: rounds between proposals (1 = after every round)")
     ap.add_argument("--ttt-batch-rounds", type=int, default=256,
                     help="batched neural PT: plain rounds that collect each network's training set (8 per round)")
+    ap.add_argument("--item-form", type=int, default=0, choices=[0, 1, 2],
+                    help="sparse workloads: 0 = the engine's choice, 1 = sliced-ELL gather, 2 = unit-regular form")
+    ap.add_argument("--positions-per-item", type=int, default=0, choices=[0, 1, 2, 4, 8],
+                    help="sparse workloads: positions per item (0 = the engine's choice)")
     ap.add_argument("--rounds", type=int, default=0,
                     help="override the rounds per step (profiling of a short case; the line then says so)")
-    ap.add_argument("--call-latency", action="store_true",
-                    help="time one small solve()-style call: in-process drop-in vs the subprocess + file boundary")
-    ap.add_argument("--shape-table", action="store_true",
-                    help="sparse engine: us per sweep of small problems for each round-end form and item size")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="default workload: skip the other workloads' lines (the 'secondary' object)")
     args = ap.parse_args()
-    if args.call_latency:
-        call_latency(args)
-    elif args.shape_table:
-        shape_table(args)
-    elif args.impl == "reference":
+    if args.impl == "reference":
         bench_reference(args)
     elif args.impl == "reference-gpu":
         bench_reference_gpu(args)
-    elif args.workload == "batched_er":
+    else:
+        run_workload(args)
+
+
+def run_workload(args):
+    if args.workload == "batched_er":
         bench_batched(args)
     elif args.workload == "sk512":
         bench_sk(args)

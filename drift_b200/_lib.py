@@ -19,12 +19,12 @@ EXPORTED = (
     "drift_pt_version", "drift_pt_last_error", "drift_pt_greedy_coloring", "drift_pt_color_order",
     "drift_pt_layout_query", "drift_pt_layout_fill", "drift_pt_thresholds", "drift_pt_workspace_bytes",
     "drift_pt_init", "drift_pt_run", "drift_pt_check", "drift_pt_energy_fp64", "drift_pt_solve",
-    "drift_pt_run_noalloc", "drift_pt_batch_items", "drift_pt_batch_init", "drift_pt_batch_workspace_bytes",
+    "drift_pt_run_noalloc", "drift_pt_noalloc_check", "drift_pt_batch_items", "drift_pt_batch_init", "drift_pt_batch_workspace_bytes",
     "drift_pt_batch_run", "drift_pt_ms_workspace_bytes", "drift_pt_ms_init", "drift_pt_ms_run",
     "drift_pt_sk_quantize", "drift_pt_sk_layout_bytes", "drift_pt_sk_layout_fill", "drift_pt_sk_scales",
     "drift_pt_sk_workspace_bytes", "drift_pt_sk_init", "drift_pt_sk_run", "drift_pt_sk_energy",
     "drift_pt_gemm_bf16", "drift_pt_made_loss", "drift_pt_made_spins_to_bf16", "drift_pt_transpose_bf16",
-    "drift_pt_colsum_bf16", "drift_pt_adam", "drift_pt_made_sample", "drift_pt_made_mh",
+    "drift_pt_colsum_bf16", "drift_pt_adam", "drift_pt_made_sample", "drift_pt_made_sample_suffix", "drift_pt_made_mh",
     "drift_pt_gms_layout_query", "drift_pt_gms_layout_fill", "drift_pt_gms_workspace_bytes", "drift_pt_gms_init",
     "drift_pt_gms_run", "drift_pt_made_group_bytes", "drift_pt_made_group_fill", "drift_pt_made_group_run",
     "drift_pt_batch_gather", "drift_pt_batch_mh", "drift_pt_batch_layout_query", "drift_pt_batch_layout_fill",
@@ -41,7 +41,8 @@ class Csr(C.Structure):
 class LayoutInfo(C.Structure):
     _fields_ = [("n", C.c_int32), ("n_pos", C.c_int32), ("n_slices", C.c_int32), ("n_colors", C.c_int32),
                 ("n_ell", C.c_int64), ("max_degree", C.c_int32), ("integer_couplings", C.c_int32),
-                ("max_field", C.c_int32), ("has_field", C.c_int32), ("min_width", C.c_int32)]
+                ("max_field", C.c_int32), ("has_field", C.c_int32), ("min_width", C.c_int32),
+                ("unit_regular", C.c_int32)]
 
 
 class Layout(C.Structure):
@@ -53,7 +54,7 @@ class DeviceProblem(C.Structure):
     _fields_ = [("n", C.c_int32), ("n_pos", C.c_int32), ("n_slices", C.c_int32), ("n_colors", C.c_int32),
                 ("integer_path", C.c_int32), ("max_field", C.c_int32), ("max_width", C.c_int32),
                 ("max_class", C.c_int32), ("has_field", C.c_int32), ("min_width", C.c_int32),
-                ("n_ell", C.c_int64),
+                ("unit_regular", C.c_int32), ("n_ell", C.c_int64),
                 ("color_ptr", vp), ("slice_off", vp), ("ell_nbr", vp), ("ell_w", vp), ("h_pos", vp)]
 
 
@@ -66,7 +67,8 @@ class RunArgs(C.Structure):
     _fields_ = [("n_replicas", C.c_int32), ("n_rounds", C.c_int32), ("sweeps_per_round", C.c_int32),
                 ("round_sync", C.c_int32), ("round_offset", C.c_int64), ("seed", C.c_uint64),
                 ("instance", C.c_uint32), ("replicas_per_cta", C.c_int32), ("threads_per_cta", C.c_int32),
-                ("positions_per_item", C.c_int32), ("betas", vp), ("thresholds", vp), ("timeout_s", C.c_double)]
+                ("positions_per_item", C.c_int32), ("item_form", C.c_int32), ("betas", vp), ("thresholds", vp),
+                ("timeout_s", C.c_double)]
 
 
 class SolveArgs(C.Structure):
@@ -128,6 +130,7 @@ def load():
                                C.c_size_t, vp]
     L.drift_pt_run_noalloc.argtypes = [C.POINTER(DeviceProblem), C.POINTER(RunArgs), C.POINTER(DeviceState), vp]
     L.drift_pt_check.argtypes = [vp, vp]
+    L.drift_pt_noalloc_check.argtypes = [vp]
     L.drift_pt_batch_items.argtypes = [C.c_int32, vp, vp, C.c_int32, C.c_int64, vp, C.POINTER(C.c_int32)]
     L.drift_pt_batch_init.argtypes = [C.POINTER(BatchProblem), C.POINTER(BatchRunArgs), C.POINTER(DeviceState), vp]
     L.drift_pt_batch_workspace_bytes.argtypes = [C.POINTER(BatchProblem), C.POINTER(C.c_size_t)]

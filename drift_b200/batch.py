@@ -247,11 +247,50 @@ class BatchEngine:
         out["best_energy"] = out["best_energy_fixed"] * sc
         return out
 
+    def capture_job(self, n_rounds: int, launch_rounds: int = 0) -> "JobGraph":
+        """A whole job captured as one CUDA graph: the initialisation and n_rounds rounds, as
+        launches of launch_rounds rounds each (0: one launch). Replaying it runs the job from the
+        start with this engine's seed, so every replay gives the same bits as `init(); run(n_rounds)`."""
+        return JobGraph(self, n_rounds, launch_rounds)
+
     def best_energies(self) -> np.ndarray:
         """Lowest energy of every instance so far (model units)."""
         be = self.best_energy.cpu().numpy()
         return np.array([be[int(d["slot0"]):int(d["slot0"]) + int(d["n_replicas"])].min() for d in self.bp.desc]) \
             * self.bp.energy_scale()
+
+
+class JobGraph:
+    """A batched PT job (drift_pt_batch_init plus every round) captured once as a CUDA graph, so a
+    whole run is one graph launch. The engine's kernel attributes are set by one eager round before
+    the capture (no attribute or occupancy call is made inside it); the state buffers are the
+    engine's own, and the graph writes them on every replay."""
+
+    def __init__(self, eng: BatchEngine, n_rounds: int, launch_rounds: int = 0):
+        torch = eng.torch
+        if n_rounds < 1:
+            raise ValueError("a job has at least one round")
+        self.eng, self.n_rounds = eng, int(n_rounds)
+        step = int(launch_rounds) if launch_rounds > 0 else self.n_rounds
+        eng.init()
+        eng.run(1)  # outside the capture: kernel attributes, the launch plan's caches
+        torch.cuda.synchronize(eng.bp.device)
+        self.launches = 0
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            eng.init()
+            done = 0
+            while done < self.n_rounds:
+                c = min(step, self.n_rounds - done)
+                eng.run(c)
+                done += c
+                self.launches += 1
+        eng.rounds_done = self.n_rounds
+
+    def replay(self) -> None:
+        """Run the whole job again (asynchronously on the current stream)."""
+        self.graph.replay()
+        self.eng.rounds_done = self.n_rounds
 
 
 _TUNE_CACHE: dict = {}

@@ -166,6 +166,7 @@ namespace {
 struct LaunchPlan {
   int rpc, threads, in_smem, grid, p;
   int cluster;  // > 0: the grid is one cluster of this many CTAs
+  int unit;     // 1: the unit-regular item form
   size_t smem;
 };
 
@@ -223,8 +224,8 @@ int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPl
   };
   // positions per item (8, 4 or 1; the fp32 path always uses 8); 0 = chosen below
   const int P_user = r->positions_per_item;
-  if (P_user != 0 && P_user != 8 && P_user != 4 && P_user != 1)
-    return set_error(DRIFT_PT_EINVAL, "positions_per_item must be 0, 1, 4 or 8");
+  if (P_user != 0 && P_user != 8 && P_user != 4 && P_user != 2 && P_user != 1)
+    return set_error(DRIFT_PT_EINVAL, "positions_per_item must be 0, 1, 2, 4 or 8");
   // threads per slot: one per item of the largest colour class (32-group runs times 8/P
   // sub-blocks), as a power of two below 32 or a multiple of 32, with rpc * tps a multiple of 32
   // and at most kMaxThreads (0 = none)
@@ -258,6 +259,84 @@ int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPl
   const int mode = r->round_sync;
   if (mode < 0 || mode > 2) return set_error(DRIFT_PT_EINVAL, "round_sync must be 0 (auto), 1 (grid) or 2 (cluster)");
   lp->cluster = 0;
+  lp->unit = 0;
+
+  // ---- the unit-regular form: one replica slot per CTA, 8 positions per item, neighbour addresses
+  // and the decision table staged in shared memory (problems whose spins all have W couplings of
+  // +-1 and no field) ----
+  const int form = r->item_form;
+  if (form < 0 || form > 2) return set_error(DRIFT_PT_EINVAL, "item_form must be 0 (auto), 1 (gather) or 2 (unit)");
+  const bool unit_ok = ip && p->unit_regular && !p->has_field && p->max_width == p->min_width &&
+                       p->max_field == p->max_width && unit_width_supported(p->max_width) &&
+                       r->replicas_per_cta <= 1 && (P_user == 0 || P_user == 2 || P_user == 4) &&
+                       p->n_colors <= kUnitPhases && 2 * (long long)p->n_pos + 16 <= 65536 &&
+                       (p->max_class + 14) / kGroup * 2 <= kMaxUnitThreads;
+  if (form == 2 && !unit_ok)
+    return set_error(DRIFT_PT_EUNSUPPORTED,
+                     "item_form 2 needs a unit-regular problem (every spin with the same number, 2, 3, 4 or 6, of "
+                     "+-1 couplings, no field, at most 32760 positions, at most 4 colour classes of at most 4080 "
+                     "spins), one replica per CTA and 2 or 4 positions per item");
+  if (P_user == 2 && (!unit_ok || form == 1))
+    return set_error(DRIFT_PT_EINVAL, "positions_per_item 2 exists in the unit-regular form only");
+  LaunchPlan unit_grid{};
+  bool have_unit_grid = false;
+  if (unit_ok && form != 1) {
+    const int W = p->max_width;
+    // items of the largest colour class: a class of m positions touches at most (m + 14) / 8 groups
+    auto items_of = [&](int P_) { return ((p->max_class + 14) / kGroup) * (kGroup / P_); };
+    const int PU = P_user ? P_user : (items_of(2) <= unit_max_threads(2) ? 2 : 4);
+    auto total_u = [&](int threads_, bool cl) {
+      return smem_layout(p->n_pos, 1, R, p->max_field, p->n_colors, p->n_slices, p->n_ell, true, true, threads_, cl,
+                         W, PU)
+          .total;
+    };
+    // one item per thread and colour phase (the kernel's static schedule)
+    const int threads = r->threads_per_cta > 0 ? r->threads_per_cta : ((items_of(PU) + 31) / 32) * 32;
+    if (threads >= items_of(PU) && threads <= unit_max_threads(PU) && threads % 32 == 0) {
+      if (mode != 1 && R >= 2 && R <= kMaxCluster && total_u(threads, true) <= (size_t)di.max_smem_optin) {
+        const void* fn = run_kernel_ptr(ip, 1, W, W, 0, PU, 1, 1);
+        const size_t smem = total_u(threads, true);
+        int per_sm = 0;
+        bool ok = false;
+        rc = prepare_kernel(fn, threads, smem, &per_sm);
+        if (rc) return rc;
+        rc = cluster_fits(fn, R, threads, smem, &ok);
+        if (rc) return rc;
+        if (ok) {
+          *lp = LaunchPlan{1, threads, 1, R, PU, R, 1, smem};
+          return DRIFT_PT_OK;
+        }
+      }
+      if (mode != 2 && total_u(threads, false) <= (size_t)di.max_smem_optin) {
+        const void* fn = run_kernel_ptr(ip, 1, W, W, 0, PU, 0, 1);
+        const size_t smem = total_u(threads, false);
+        int per_sm = 0;
+        rc = prepare_kernel(fn, threads, smem, &per_sm);
+        if (rc) return rc;
+        if ((long long)per_sm * di.sm_count >= R) {
+          unit_grid = LaunchPlan{1, threads, 1, R, PU, 0, 1, smem};
+          have_unit_grid = true;
+          // chosen here unless the automatic shape may still pick a cluster form below (small
+          // ladders, where the cluster form's shorter round end is worth more than the item form)
+          if (form == 2 || mode == 1 || R > 2 * kMaxCluster) {
+            *lp = unit_grid;
+            return DRIFT_PT_OK;
+          }
+        }
+      }
+    }
+    if (form == 2)
+      return set_error(DRIFT_PT_EUNSUPPORTED, "item_form 2: no launch shape with one replica per CTA fits (%d replicas, "
+                       "%d positions, round_sync %d)", R, p->n_pos, mode);
+  }
+  // the unit-regular grid form when no cluster form of the gather is taken (automatic shape only)
+  auto unit_or = [&](auto&& other) -> int {
+    if (have_unit_grid) {
+      *lp = unit_grid;
+      return DRIFT_PT_OK;
+    }
+    return other();
+  };
 
   // ---- the cluster form: the ladder in one cluster of at most 16 CTAs, coupling table in shared
   // memory; a round's energies cross through distributed shared memory behind one barrier ----
@@ -374,11 +453,10 @@ int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPl
     rc = try_cluster(1, true, &done);
     if (rc || done) return rc;
   }
-  if (p1_alone && R <= di.sm_count && phases >= 4) return plan_grid(1);
+  if (p1_alone && R <= di.sm_count && phases >= 4) return unit_or([&] { return plan_grid(1); });
   rc = try_cluster(4, true, &done);
   if (rc || done) return rc;
-  return plan_grid(p1_alone && R <= di.sm_count ? 1 : 4);
-  return DRIFT_PT_OK;
+  return unit_or([&] { return plan_grid(p1_alone && R <= di.sm_count ? 1 : 4); });
 }
 
 }  // namespace
@@ -437,7 +515,7 @@ extern "C" int drift_pt_run(const DriftPtDeviceProblem* prob, const DriftPtRunAr
   cfg.numAttrs = 1;
   void* kargs[] = {&a};
   e = cudaLaunchKernelExC(&cfg, run_kernel_ptr(prob->integer_path, lp.in_smem, prob->max_width, prob->min_width,
-                                                prob->has_field, lp.p, lp.cluster > 0 ? 1 : 0),
+                                                prob->has_field, lp.p, lp.cluster > 0 ? 1 : 0, lp.unit),
                           kargs);
   if (e != cudaSuccess) return cuda_fail(e, "pt_run_kernel launch");
   return DRIFT_PT_OK;
@@ -566,6 +644,7 @@ extern "C" int drift_pt_solve(const DriftPtCsr* csr, const DriftPtSolveArgs* arg
   prob.max_field = info.max_field;
   prob.max_width = info.max_degree;
   prob.min_width = info.min_width;
+  prob.unit_regular = ip ? info.unit_regular : 0;
   prob.max_class = max_class;
   prob.has_field = info.has_field;
   prob.n_ell = info.n_ell;

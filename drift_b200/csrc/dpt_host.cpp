@@ -182,6 +182,14 @@ extern "C" int drift_pt_layout_query(const DriftPtCsr* csr, DriftPtLayoutInfo* i
     }
   info->integer_couplings = integer ? 1 : 0;
   info->max_field = integer ? (int32_t)std::max<int64_t>(F, 1) : 0;
+  // unit-regular: every spin has exactly max_degree couplings, each +1 or -1, and no field
+  bool unit = integer && !info->has_field && maxdeg >= 1;
+  for (int32_t i = 0; i < n && unit; ++i) {
+    if (csr->row_ptr[i + 1] - csr->row_ptr[i] != maxdeg) unit = false;
+    for (int32_t t = csr->row_ptr[i]; t < csr->row_ptr[i + 1] && unit; ++t)
+      if (std::fabs(csr->weight[t]) != 1.0f) unit = false;
+  }
+  info->unit_regular = unit ? 1 : 0;
   return DRIFT_PT_OK;
 }
 

@@ -13,6 +13,12 @@ constexpr int kGroup = 8;
 constexpr int kSlicePositions = 256;
 // Largest CTA of the sweep kernel: 512 threads leave 128 registers per thread for the gathers.
 constexpr int kMaxThreads = 512;
+// Largest CTA of the unit-regular form: 832 threads with 2 positions per item (72 registers per
+// thread), 1024 with 4 (64 registers).
+constexpr int kMaxUnitThreads = 1024;
+constexpr int unit_max_threads(int P) { return P == 2 ? 832 : 1024; }
+// Colour classes the unit-regular form schedules statically (one register pair per class).
+constexpr int kUnitPhases = 4;
 
 int set_error(int code, const char* fmt, ...);
 void clear_error();

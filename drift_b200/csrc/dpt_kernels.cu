@@ -88,13 +88,22 @@ __device__ __forceinline__ int ld_relaxed_i32(const int* p) {
 // ---------------------------------------------------------------------------------------------
 // kCluster: the grid is one cluster (CTA rank = blockIdx.x) and the round's energies are exchanged
 // through distributed shared memory behind one cluster barrier instead of global memory.
-template <bool kInt, bool kInSmem, int W, bool kExactW, bool kField, int P, bool kCluster>
-__global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelArgs a) {
-  static_assert(P == 8 || (kInt && (P == 4 || P == 1)), "positions per item");
+// kUnitW > 0: the unit-regular form (every spin has kUnitW couplings of +-1, no field; one
+// replica slot per CTA; P = 2 or 4 positions per item, up to kMaxUnitThreads threads): items read
+// 16-bit neighbour addresses from a table staged at launch instead of gathering the sliced ELL,
+// spins live as 0/1 bytes with a flipped copy, and each group's Philox block is computed once per
+// sweep, a sweep ahead, into shared memory (item_unit).
+template <bool kInt, bool kInSmem, int W, bool kExactW, bool kField, int P, bool kCluster, int kUnitW = 0>
+__global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads, 1) pt_run_kernel(const PtKernelArgs a) {
+  constexpr bool kUnit = kUnitW > 0;
+  static_assert(kUnit || P == 8 || (kInt && (P == 4 || P == 1)), "positions per item");
+  static_assert(!kUnit || (kInt && kInSmem && !kField && (P == 2 || P == 4)), "unit-regular form");
   constexpr int NB = kGroup / P;  // items per group
   unsigned char* smem = dpt_smem;
   const SmemLayout L = smem_layout(a.n_pos, a.rpc, a.R, a.F, a.n_colors, a.n_slices, a.n_ell, kInt, kInSmem,
-                                   (int)blockDim.x, kCluster);
+                                   (int)blockDim.x, kCluster, kUnitW, kUnit ? P : 2);
+  // bytes of one slot's spins in shared memory
+  const uint32_t sp_stride = kUnit ? (uint32_t)unit_slot_bytes(a.n_pos) : (uint32_t)a.n_pos;
   long long* cpub = reinterpret_cast<long long*>(smem + L.cpub);
   int8_t* sp = reinterpret_cast<int8_t*>(smem + L.spins);
   long long* eacc = reinterpret_cast<long long*>(smem + L.eacc);
@@ -117,7 +126,23 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelAr
   const int nloc = min(a.rpc, R - s0);
 
   // ---- stage state and tables ----
-  {
+  if constexpr (kUnit) {
+    // +1 -> 0 and -1 -> 1 (the sign bit of each byte), the flipped copy, and 16 zero bytes
+    const int chunks = n_pos / 16;
+    const uint4* src = reinterpret_cast<const uint4*>(a.spins + (size_t)s0 * n_pos);
+    for (int i = tid; i < nloc * chunks; i += B) {
+      const int sl = i / chunks, c = i - sl * chunks;
+      const uint4 v = src[i];
+      const uint4 b = make_uint4((v.x >> 7) & 0x01010101u, (v.y >> 7) & 0x01010101u, (v.z >> 7) & 0x01010101u,
+                                 (v.w >> 7) & 0x01010101u);
+      unsigned char* base = smem + L.spins + (size_t)sl * sp_stride;
+      *reinterpret_cast<uint4*>(base + 16 * c) = b;
+      *reinterpret_cast<uint4*>(base + n_pos + 16 * c) =
+          make_uint4(b.x ^ 0x01010101u, b.y ^ 0x01010101u, b.z ^ 0x01010101u, b.w ^ 0x01010101u);
+    }
+    for (int i = tid; i < nloc; i += B)
+      *reinterpret_cast<uint4*>(smem + L.spins + (size_t)i * sp_stride + 2 * n_pos) = make_uint4(0, 0, 0, 0);
+  } else {
     const int4* src = reinterpret_cast<const int4*>(a.spins + (size_t)s0 * n_pos);
     int4* dst = reinterpret_cast<int4*>(sp);
     const int nv = nloc * n_pos / 16;
@@ -133,7 +158,17 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelAr
     slot_sm[i] = a.slot_of_rung[i];
     beta_sm[i] = a.betas[i];
   }
-  if constexpr (kInt) {
+  if constexpr (kUnit) {
+    // decision table: entry (rung, b, k) = (x << 32) | threshold of x, x = (1 - 2b)(W - 2k)
+    constexpr int row = 2 * (kUnitW + 1);
+    unsigned long long* tab = reinterpret_cast<unsigned long long*>(smem + L.thr);
+    for (int i = tid; i < R * row; i += B) {
+      const int r = i / row, j = i - r * row, bb = j / (kUnitW + 1), kk = j - bb * (kUnitW + 1);
+      const int x = (1 - 2 * bb) * (kUnitW - 2 * kk);
+      const uint32_t th = x >= 1 ? a.thr[r * a.F + x - 1] : 0xFFFFFFFFu;
+      tab[i] = ((unsigned long long)(uint32_t)x << 32) | th;
+    }
+  } else if constexpr (kInt) {
     // extended rows: entry x + F for x = -F..F; x <= 0 never reads its entry (always accepted)
     const int row = 2 * a.F + 1;
     for (int i = tid; i < R * row; i += B) {
@@ -153,7 +188,34 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelAr
   T.w8 = static_cast<const int8_t*>(a.ell_w);
   T.wf = static_cast<const float*>(a.ell_w);
   T.h = a.h_pos;
-  if constexpr (kInSmem) {
+  if constexpr (kUnit) {
+    // neighbour-address rows, one per item of P positions: entry i W + d is the 16-bit address of
+    // the byte neighbour d of position P item + i contributes, in the slot's b array (+1 coupling)
+    // or b ^ 1 array (-1 coupling); padding entries (weight 0, on padding positions only) point at
+    // the zero bytes behind the two arrays. The spins start at shared offset 0 (one slot per CTA),
+    // so every address is below 2 n_pos + 16 <= 2^16.
+    constexpr int RB = ((2 * P * kUnitW + 7) / 8) * 8;
+    uint16_t* desc = reinterpret_cast<uint16_t*>(smem + L.nbr);
+    const int8_t* w8 = static_cast<const int8_t*>(a.ell_w);
+    const uint32_t base = (uint32_t)L.spins;
+    for (int i = tid; i < kUnitW * n_pos; i += B) {
+      const int p = i / kUnitW, d = i - p * kUnitW;
+      const int S = p >> 8, lane = (p >> 3) & 31, q = p & 7;
+      const long long e = (long long)(S * kUnitW + d) * kSlicePositions + q * 32 + lane;
+      const int wt = w8[e];
+      const uint32_t at = wt == 0 ? base + 2u * (uint32_t)n_pos
+                                  : base + (wt < 0 ? (uint32_t)n_pos : 0u) + (uint32_t)a.ell_nbr[e];
+      desc[(size_t)(p / P) * (RB / 2) + (p % P) * kUnitW + d] = (uint16_t)at;
+    }
+    // the Philox blocks of the launch's first sweep (the items compute each later sweep's ahead)
+    const uint32_t t0 = (uint32_t)(a.round0 * a.spr);
+    uint4* ub = reinterpret_cast<uint4*>(smem + L.w + 16 * (size_t)(n_pos / kGroup) * (t0 & 1u));
+    const uint32_t c_sw = ctr3(kTagSweep, a.inst);
+    for (int g = tid; g < n_pos / kGroup; g += B) {
+      const U4 u = philox(U4{(uint32_t)g, t0, (uint32_t)s0, c_sw}, a.k0, a.k1);
+      ub[g] = make_uint4(u.x, u.y, u.z, u.w);
+    }
+  } else if constexpr (kInSmem) {
     int* soff_sm = reinterpret_cast<int*>(smem + L.soff);
     for (int i = tid; i <= a.n_slices; i += B) soff_sm[i] = a.slice_off[i];
     if constexpr (kInt) {
@@ -194,19 +256,61 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelAr
   const int my_sl = tid / tps, lt = tid - my_sl * tps;
   const bool active = my_sl < nloc;
   const int my_slot = s0 + (active ? my_sl : 0);
-  const uint32_t my_sp_o = (uint32_t)L.spins + (uint32_t)(active ? my_sl : 0) * (uint32_t)n_pos;
+  const uint32_t my_sp_o = (uint32_t)L.spins + (uint32_t)(active ? my_sl : 0) * sp_stride;
   const int k = a.n_colors;
   const uint32_t c_sweep = ctr3(kTagSweep, a.inst), c_second = ctr3(kTagSecond, a.inst);
+  // Unit-regular form: each thread's work in each colour phase is the same every sweep, so it is
+  // fixed here once: item lt of the class (item index | in-class mask << 16 | 1 << 31, or 0) and the
+  // group whose next-sweep Philox block the thread computes (group + 1, or 0): the groups whose first
+  // position lies in the class, taken by the CTA's last threads. (Moving all blocks to the phases
+  // with the most idle threads instead measured slower on MaxCut N = 4096: the small phases became
+  // issue-bound, while in the large phases the blocks overlap other warps' items.) The host makes
+  // the CTA wide enough for one item per thread and phase.
+  uint32_t s_item[kUnitPhases], s_px[kUnitPhases];
+#pragma unroll
+  for (int c = 0; c < kUnitPhases; ++c) {
+    s_item[c] = 0u;
+    s_px[c] = 0u;
+    if (kUnit && c < k) {
+      const int lo = cptr[c], hi = cptr[c + 1];
+      const int glo = lo >> 3, ghi = (hi + 7) >> 3;
+      if (lt < (ghi - glo) * NB) {
+        const uint32_t item = (uint32_t)(glo * NB + lt);
+        const uint32_t msk = range_mask<P>((int)item * P, lo, hi);
+        s_item[c] = msk ? (item | (msk << 16) | 0x80000000u) : 0u;
+      }
+      const int gp = (lo + 7) / kGroup + (tps - 1 - lt);
+      if (gp < (hi + 7) / kGroup) s_px[c] = (uint32_t)gp + 1u;
+    }
+  }
   for (int j = 0; j < a.n_rounds; ++j) {
     const long long round = a.round0 + j;
     long long dacc = 0;
-    const uint32_t thr_o = kInt ? (uint32_t)L.thr + 4u * (uint32_t)(rung_sm[my_slot] * (2 * a.F + 1) + a.F) : 0u;
+    const uint32_t thr_o = kUnit ? (uint32_t)L.thr + 16u * (uint32_t)(rung_sm[my_slot] * (kUnitW + 1))
+                           : kInt ? (uint32_t)L.thr + 4u * (uint32_t)(rung_sm[my_slot] * (2 * a.F + 1) + a.F) : 0u;
     const float neg2beta = kInt ? 0.0f : nb_sm[active ? my_sl : 0];
     // the class bounds never change during the launch: each phase reads the next phase's before
     // its barrier, so no shared load starts the phase after it
     int lo_n = cptr[0], hi_n = cptr[1];
     for (int sw = 0; sw < a.spr; ++sw) {
       const uint32_t t = (uint32_t)(round * a.spr + sw);
+      if constexpr (kUnit) {
+        // the static schedule: at most one item and one next-sweep Philox block per thread and phase
+        const uint32_t ng = (uint32_t)(n_pos / kGroup);
+        const uint32_t ubuf = (uint32_t)L.w + 16u * ng * (t & 1u), unext = (uint32_t)L.w + 16u * ng * ((t + 1u) & 1u);
+#pragma unroll
+        for (int c = 0; c < kUnitPhases; ++c) {
+          if (c < k) {
+            if (s_px[c]) unit_next_block(s_px[c] - 1u, t, (uint32_t)my_slot, unext, c_sweep, a.k0, a.k1);
+            if (s_item[c] >> 31)
+              dacc += item_unit<kUnitW, P>(s_item[c] & 0xFFFFu, (s_item[c] >> 16) & 0xFu, t, (uint32_t)my_slot,
+                                           my_sp_o, my_sp_o + (uint32_t)n_pos, (uint32_t)L.nbr, ubuf, thr_o,
+                                           c_second, a.k0, a.k1);
+            __syncthreads();
+          }
+        }
+        continue;
+      }
       for (int c = 0; c < k; ++c) {
         const int lo = lo_n, hi = hi_n;
         {
@@ -215,20 +319,22 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelAr
           hi_n = cptr[cn + 1];
         }
         const int glo = lo >> 3, ghi = (hi + 7) >> 3;
-        // item v -> (group, sub-block): 32 consecutive items are 32 consecutive groups (coalesced
-        // coupling reads), the NB sub-blocks of those groups follow as the next 32-item runs
-        const int span = ((ghi - glo + 31) >> 5) * 32 * NB;
-        if (active) {
-          for (int v = lt; v < span; v += tps) {
-            const int b = (v >> 5) & (NB - 1);
-            const int g = glo + (v / (32 * NB)) * 32 + (v & 31);
-            if (g >= ghi) continue;
-            if constexpr (kInt)
-              dacc += group_int<W, kExactW, kInSmem, kField, P>(g, b, lo, hi, t, (uint32_t)my_slot, my_sp_o, T,
-                                                                thr_o, c_sweep, c_second, a.k0, a.k1);
-            else
-              dacc += group_f32<W, kExactW, kInSmem, kField>(g, lo, hi, t, (uint32_t)my_slot, my_sp_o, T, neg2beta,
-                                                             c_sweep, c_second, a.k0, a.k1);
+        if constexpr (!kUnit) {
+          // item v -> (group, sub-block): 32 consecutive items are 32 consecutive groups (coalesced
+          // coupling reads), the NB sub-blocks of those groups follow as the next 32-item runs
+          const int span = ((ghi - glo + 31) >> 5) * 32 * NB;
+          if (active) {
+            for (int v = lt; v < span; v += tps) {
+              const int b = (v >> 5) & (NB - 1);
+              const int g = glo + (v / (32 * NB)) * 32 + (v & 31);
+              if (g >= ghi) continue;
+              if constexpr (kInt)
+                dacc += group_int<W, kExactW, kInSmem, kField, P>(g, b, lo, hi, t, (uint32_t)my_slot, my_sp_o, T,
+                                                                  thr_o, c_sweep, c_second, a.k0, a.k1);
+              else
+                dacc += group_f32<W, kExactW, kInSmem, kField>(g, lo, hi, t, (uint32_t)my_slot, my_sp_o, T,
+                                                               neg2beta, c_sweep, c_second, a.k0, a.k1);
+            }
           }
         }
         __syncthreads();
@@ -248,10 +354,15 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelAr
     for (int off = seg >> 1; off > 0; off >>= 1) dacc += __shfl_xor_sync(0xffffffffu, dacc, off);
     if (lt % seg == 0) eacc[tid / seg] = dacc;
     __syncthreads();
-    for (int i = tid; i < nloc; i += B) {
-      long long e = ecur[i];
-      const int nseg = tps / seg;
-      for (int q = 0; q < nseg; ++q) e += eacc[i * nseg + q];
+    // a slot's nseg <= 32 partial sums are added by one warp (shuffles, not a serial chain of
+    // shared loads); slots are spread over the warps. Integer sums: any order gives the same bits.
+    const int nseg = tps / seg;
+    for (int i = tid >> 5; i < nloc; i += B >> 5) {
+      const int ln = tid & 31;
+      long long part = ln < nseg ? eacc[i * nseg + ln] : 0ll;
+      for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
+      if (ln == 0) {
+      const long long e = ecur[i] + part;
       ecur[i] = e;
       imp[i] = (e < ebest[i]) ? 1 : 0;
       if (e < ebest[i]) ebest[i] = e;
@@ -269,6 +380,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelAr
           st_release_u64(a.tags + at, (unsigned long long)round + 1ull);
         }
       }
+      }
     }
     if constexpr (kCluster) {
       // one cluster barrier publishes this round's energies to the other CTAs and, being a barrier
@@ -278,7 +390,19 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelAr
     } else {
       __syncthreads();
     }
-    {
+    if constexpr (kUnit) {
+      // the same copy from the 0/1 bytes (b -> 1 - 2b: 0 -> 0x01, 1 -> 0xFF)
+      const int chunks = n_pos / 16;
+      uint4* dst = reinterpret_cast<uint4*>(a.best_spins + (size_t)s0 * n_pos);
+      for (int i = tid; i < nloc * chunks; i += B) {
+        const int sl = i / chunks;
+        if (imp[sl]) {
+          const uint4 v = *reinterpret_cast<const uint4*>(sp + (size_t)sl * sp_stride + 16 * (i - sl * chunks));
+          dst[i] = make_uint4((v.x * 0xFEu) ^ 0x01010101u, (v.y * 0xFEu) ^ 0x01010101u, (v.z * 0xFEu) ^ 0x01010101u,
+                              (v.w * 0xFEu) ^ 0x01010101u);
+        }
+      }
+    } else {
       // copy the spins of every slot that reached a new best, all slots in one pass
       const int chunks = n_pos / 16;
       const int4* src = reinterpret_cast<const int4*>(sp);
@@ -398,7 +522,16 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pt_run_kernel(const PtKernelAr
   // cluster form: no CTA leaves while another may still read its last round's energies
   if constexpr (kCluster) cl_sync_full();
   __syncthreads();
-  {
+  if constexpr (kUnit) {
+    const int chunks = n_pos / 16;
+    uint4* dst = reinterpret_cast<uint4*>(a.spins + (size_t)s0 * n_pos);
+    for (int i = tid; i < nloc * chunks; i += B) {
+      const int sl = i / chunks;
+      const uint4 v = *reinterpret_cast<const uint4*>(sp + (size_t)sl * sp_stride + 16 * (i - sl * chunks));
+      dst[i] = make_uint4((v.x * 0xFEu) ^ 0x01010101u, (v.y * 0xFEu) ^ 0x01010101u, (v.z * 0xFEu) ^ 0x01010101u,
+                          (v.w * 0xFEu) ^ 0x01010101u);
+    }
+  } else {
     const int4* src = reinterpret_cast<const int4*>(sp);
     int4* dst = reinterpret_cast<int4*>(a.spins + (size_t)s0 * n_pos);
     const int nv = nloc * n_pos / 16;
@@ -594,10 +727,29 @@ static const void* pick_p(int max_w, int min_w, int p) {
   return pick_w<kInt, kInSmem, kField, 8, kCl>(max_w, min_w);
 }
 
+template <bool kCl, int P>
+static const void* pick_unit(int w) {
+  switch (w) {
+    case 2: return (const void*)pt_run_kernel<true, true, 2, true, false, P, kCl, 2>;
+    case 3: return (const void*)pt_run_kernel<true, true, 3, true, false, P, kCl, 3>;
+    case 4: return (const void*)pt_run_kernel<true, true, 4, true, false, P, kCl, 4>;
+    case 6: return (const void*)pt_run_kernel<true, true, 6, true, false, P, kCl, 6>;
+    default: return nullptr;
+  }
+}
+
+bool unit_width_supported(int w) { return w == 2 || w == 3 || w == 4 || w == 6; }
+
 // The cluster form exists with the coupling table in shared memory only (small problems, where the
 // round end is a large share of the round).
 const void* run_kernel_ptr(int integer_path, int in_smem, int max_width, int min_width, int has_field,
-                           int positions_per_item, int cluster) {
+                           int positions_per_item, int cluster, int unit) {
+  if (unit) {
+    if (!integer_path || has_field || max_width != min_width) return nullptr;
+    if (positions_per_item == 2) return cluster ? pick_unit<true, 2>(max_width) : pick_unit<false, 2>(max_width);
+    if (positions_per_item == 4) return cluster ? pick_unit<true, 4>(max_width) : pick_unit<false, 4>(max_width);
+    return nullptr;
+  }
   const int p = positions_per_item, w = max_width, m = min_width;
   if (cluster) {
     if (!in_smem) return nullptr;

@@ -121,7 +121,8 @@ __global__ void adam_kernel(int rows, int cols, float* w, const float* g, float*
 // sampling / evaluation: one CTA per group of S samples, units processed in degree order
 // ------------------------------------------------------------------------------------------------
 struct MadeArgs {
-  int n, h1, h2, S, count, mode;  // mode 0: sample x, 1: evaluate given x
+  int n, h1, h2, S, count, mode;  // mode 0: sample x, 1: evaluate given x, 2: keep x_<keep, draw the rest
+  int keep;
   const __nv_bfloat16* w1t;       // [n][h1]   column i of W1 = row i
   const __nv_bfloat16* w2t;       // [h1][h2]
   const __nv_bfloat16* w3t;       // [h2][n]
@@ -210,7 +211,7 @@ __device__ __forceinline__ void made_sample_body(const MadeArgs& a) {
     if (tid < ns) {
       const float l = lnext[tid];
       float sv;
-      if (a.mode == 0) {
+      if (a.mode == 0 || (a.mode == 2 && i >= a.keep)) {
         const U4 u = philox(U4{(uint32_t)i, (uint32_t)(base + tid), a.stream, ctr3(kTagMadeSample, 0)}, a.k0, a.k1);
         const float uf = (float)(u.x >> 8) * 0x1.0p-24f;
         sv = uf < 1.0f / (1.0f + expf(-l)) ? 1.0f : -1.0f;
@@ -427,14 +428,30 @@ extern "C" int drift_pt_adam(int32_t rows, int32_t cols, float* w, const float* 
   return made_fail("adam_kernel");
 }
 
+static int made_sample_launch(const DriftPtMadeNet* net, int32_t count, int32_t mode, int32_t keep, int8_t* x,
+                              float* logq, uint64_t seed, uint32_t stream_id, void* stream);
+
 extern "C" int drift_pt_made_sample(const DriftPtMadeNet* net, int32_t count, int32_t mode, int8_t* x, float* logq,
                                     uint64_t seed, uint32_t stream_id, void* stream) {
   clear_error();
+  if (mode != 0 && mode != 1) return set_error(DRIFT_PT_EINVAL, "made_sample: mode must be 0 or 1");
+  return made_sample_launch(net, count, mode, 0, x, logq, seed, stream_id, stream);
+}
+
+extern "C" int drift_pt_made_sample_suffix(const DriftPtMadeNet* net, int32_t count, int32_t keep, int8_t* x,
+                                           float* logq, uint64_t seed, uint32_t stream_id, void* stream) {
+  clear_error();
+  if (!net || keep < 0 || keep > net->n) return set_error(DRIFT_PT_EINVAL, "made_sample_suffix: keep must be in [0, n]");
+  return made_sample_launch(net, count, 2, keep, x, logq, seed, stream_id, stream);
+}
+
+static int made_sample_launch(const DriftPtMadeNet* net, int32_t count, int32_t mode, int32_t keep, int8_t* x,
+                              float* logq, uint64_t seed, uint32_t stream_id, void* stream) {
   if (!net || !net->w1t || !net->w2t || !net->w3t || !net->b1 || !net->b2 || !net->b3 || !net->ord1 || !net->off1 ||
       !net->ord2 || !net->off2 || !x || !logq)
     return set_error(DRIFT_PT_EINVAL, "made_sample: null argument");
-  if (net->n < 2 || net->h1 < 1 || net->h2 < 1 || count < 1 || (mode != 0 && mode != 1))
-    return set_error(DRIFT_PT_EINVAL, "made_sample: bad sizes or mode");
+  if (net->n < 2 || net->h1 < 1 || net->h2 < 1 || count < 1)
+    return set_error(DRIFT_PT_EINVAL, "made_sample: bad sizes");
   if (net->max_units_per_degree > 4) return set_error(DRIFT_PT_EINVAL, "made_sample: at most 4 hidden units per degree");
   MadeArgs a;
   std::memset(&a, 0, sizeof a);
@@ -443,6 +460,7 @@ extern "C" int drift_pt_made_sample(const DriftPtMadeNet* net, int32_t count, in
   a.h2 = net->h2;
   a.count = count;
   a.mode = mode;
+  a.keep = keep;
   a.w1t = static_cast<const __nv_bfloat16*>(net->w1t);
   a.w2t = static_cast<const __nv_bfloat16*>(net->w2t);
   a.w3t = static_cast<const __nv_bfloat16*>(net->w3t);

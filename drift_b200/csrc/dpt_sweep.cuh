@@ -19,6 +19,10 @@ __device__ __forceinline__ uint32_t lds_u32(uint32_t off) { return *reinterpret_
 __device__ __forceinline__ int lds_s32(uint32_t off) { return *reinterpret_cast<const int*>(dpt_smem + off); }
 __device__ __forceinline__ float lds_f32(uint32_t off) { return *reinterpret_cast<const float*>(dpt_smem + off); }
 __device__ __forceinline__ int lds_s8(uint32_t off) { return (int)*reinterpret_cast<const int8_t*>(dpt_smem + off); }
+__device__ __forceinline__ uint32_t lds_u8(uint32_t off) { return (uint32_t)*reinterpret_cast<const uint8_t*>(dpt_smem + off); }
+__device__ __forceinline__ uint64_t lds_u64(uint32_t off) { return *reinterpret_cast<const uint64_t*>(dpt_smem + off); }
+__device__ __forceinline__ uint4 lds_u128(uint32_t off) { return *reinterpret_cast<const uint4*>(dpt_smem + off); }
+__device__ __forceinline__ void sts_u64(uint32_t off, uint64_t v) { *reinterpret_cast<uint64_t*>(dpt_smem + off) = v; }
 
 struct Tables {
   // byte offsets in shared memory (tables staged in shared memory)
@@ -179,6 +183,131 @@ __device__ __forceinline__ int group_int(int g, int b, int lo, int hi, uint32_t 
   }
   *reinterpret_cast<SW*>(dpt_smem + own_o) = (SW)s8;
   return dacc;
+}
+
+__device__ __forceinline__ uint32_t lds_u16(uint32_t off) { return (uint32_t)*reinterpret_cast<const uint16_t*>(dpt_smem + off); }
+__device__ __forceinline__ void sts_u16(uint32_t off, uint32_t v) { *reinterpret_cast<uint16_t*>(dpt_smem + off) = (uint16_t)v; }
+__device__ __forceinline__ void sts_u32(uint32_t off, uint32_t v) { *reinterpret_cast<uint32_t*>(dpt_smem + off) = v; }
+__device__ __forceinline__ void sts_u128(uint32_t off, uint4 v) { *reinterpret_cast<uint4*>(dpt_smem + off) = v; }
+
+// One item of the unit-regular form: positions 8g + P j .. 8g + P j + P - 1 (P = 2 or 4) of one
+// replica slot, on a problem whose spins all have W couplings of +-1 and no field.
+//  * The slot's spins are bytes b (0 for +1, 1 for -1) at b_o and their flipped copy b ^ 1 at nb_o.
+//  * The item's row of the neighbour-address table (desc_o, unit_row_bytes(P, W) bytes per item)
+//    holds, for each position i and coupling d, the 16-bit shared address of the byte that neighbour
+//    contributes: its b for a +1 coupling, its b ^ 1 for a -1 coupling. So J s_nb = 1 - 2 byte and
+//    the position's field is W - 2k, k the sum of its W bytes.
+//  * tab_o is the slot's rung row of the decision table: entry (b, k) holds x = (1 - 2b)(W - 2k)
+//    (= s_i field_i, half the flip's energy change) and the threshold of x.
+//  * The uniforms come from the group's Philox block of this sweep, read from ubuf_o (16 bytes per
+//    group); the caller computes the next sweep's blocks separately (unit_next_block).
+// The Metropolis test, the uniforms and the energy change are those of group_int, so every form
+// runs the same chain bit for bit.
+// The item is given by its index (item = g NI + j, NI = 8 / P items per group) and the mask of its
+// positions that lie in the phase's colour class.
+template <int W, int P>
+__device__ __forceinline__ int item_unit(uint32_t item, uint32_t inmask, uint32_t t, uint32_t slot, uint32_t b_o,
+                                         uint32_t nb_o, uint32_t desc_o, uint32_t ubuf_o, uint32_t tab_o,
+                                         uint32_t c_second, uint32_t k0, uint32_t k1) {
+  static_assert(P == 2 || P == 4, "positions per item");
+  constexpr int NI = kGroup / P;
+  constexpr int RB = ((2 * P * W + 7) / 8) * 8;  // unit_row_bytes(P, W)
+  const uint32_t g = item / NI, j = item % NI;
+  const int p0 = (int)(item * P);
+  uint32_t a16[RB / 2];
+  {
+    const uint32_t row = desc_o + item * RB;
+    uint32_t w32[RB / 4];
+    if constexpr (RB % 16 == 0) {
+#pragma unroll
+      for (int c = 0; c < RB / 16; ++c) {
+        const uint4 v = lds_u128(row + 16u * c);
+        w32[4 * c] = v.x; w32[4 * c + 1] = v.y; w32[4 * c + 2] = v.z; w32[4 * c + 3] = v.w;
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < RB / 8; ++c) {
+        const uint64_t v = lds_u64(row + 8u * c);
+        w32[2 * c] = (uint32_t)v;
+        w32[2 * c + 1] = (uint32_t)(v >> 32);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < RB / 4; ++c) {
+      a16[2 * c] = w32[c] & 0xFFFFu;
+      a16[2 * c + 1] = w32[c] >> 16;
+    }
+  }
+  uint32_t nbv[P * W];
+#pragma unroll
+  for (int k = 0; k < P * W; ++k) nbv[k] = lds_u8(a16[k]);
+  const uint32_t own_o = b_o + (uint32_t)p0;
+  uint32_t own = P == 2 ? lds_u16(own_o) : lds_u32(own_o);
+  uint32_t words[P / 2];
+  if constexpr (P == 2) {
+    words[0] = lds_u32(ubuf_o + 16u * (uint32_t)g + 4u * (uint32_t)j);
+  } else {
+    const uint64_t w2 = lds_u64(ubuf_o + 16u * (uint32_t)g + 8u * (uint32_t)j);
+    words[0] = (uint32_t)w2;
+    words[1] = (uint32_t)(w2 >> 32);
+  }
+  uint32_t flips = 0u, ties = 0u;
+  int dacc = 0;
+  uint32_t kk[P];
+#pragma unroll
+  for (int i = 0; i < P; ++i) {
+    uint32_t k = 0;
+#pragma unroll
+    for (int d = 0; d < W; ++d) k += nbv[i * W + d];
+    kk[i] = k;
+  }
+#pragma unroll
+  for (int i = 0; i < P; ++i) {
+    const uint32_t b = (own >> (8 * i)) & 1u;
+    const uint64_t e = lds_u64(tab_o + 8u * (b * (uint32_t)(W + 1) + kk[i]));
+    const uint32_t thr = (uint32_t)e;
+    const int x = (int)(uint32_t)(e >> 32);
+    // position q = P j + i of the group: half q & 1 (= i & 1) of word q >> 1
+    const uint32_t prim = (words[i >> 1] >> ((i & 1) * 16)) & 0xFFFFu;
+    const uint32_t th = thr >> 16;
+    const bool in = (inmask >> i) & 1u;
+    const bool acc = in & ((x <= 0) | (prim < th));
+    flips |= (uint32_t)acc << i;
+    ties |= (uint32_t)(in & (x > 0) & (prim == th)) << i;
+    dacc += acc ? 2 * x : 0;
+  }
+  if (ties) {  // the first 16 bits tie: the second half of the uniform decides
+#pragma unroll
+    for (int i = 0; i < P; ++i)
+      if ((ties >> i) & 1u) {
+        const uint32_t b = (own >> (8 * i)) & 1u;
+        const uint64_t e = lds_u64(tab_o + 8u * (b * (uint32_t)(W + 1) + kk[i]));
+        const U4 r2 = philox(U4{(uint32_t)(p0 + i), t, slot, c_second}, k0, k1);
+        if ((r2.x & 0xFFFFu) < ((uint32_t)e & 0xFFFFu)) {
+          flips |= 1u << i;
+          dacc += 2 * (int)(uint32_t)(e >> 32);
+        }
+      }
+  }
+  if (flips) {
+    // bit i of the flips -> bit 0 of byte i (see group_int), then b and b ^ 1 stored
+    own ^= ((flips * 0x00204081u) & 0x01010101u);
+    if constexpr (P == 2) {
+      sts_u16(own_o, own);
+      sts_u16(nb_o + (uint32_t)p0, own ^ 0x0101u);
+    } else {
+      sts_u32(own_o, own);
+      sts_u32(nb_o + (uint32_t)p0, own ^ 0x01010101u);
+    }
+  }
+  return dacc;
+}
+
+// The Philox block of group g for sweep t + 1 (computed during sweep t into unext_o).
+__device__ __forceinline__ void unit_next_block(uint32_t g, uint32_t t, uint32_t slot, uint32_t unext_o,
+                                                uint32_t c_sweep, uint32_t k0, uint32_t k1) {
+  const U4 nx = philox(U4{g, t + 1u, slot, c_sweep}, k0, k1);
+  sts_u128(unext_o + 16u * g, make_uint4(nx.x, nx.y, nx.z, nx.w));
 }
 
 template <int W, bool kExactW, bool kInSmem, bool kField>

@@ -110,6 +110,7 @@ class DeviceProblem:
         self.max_class = int(np.max(np.diff(color_ptr)))
         self.max_width = int(np.max(np.diff(slice_off))) if slice_off.size > 1 else 0
         self.min_width = int(np.min(np.diff(slice_off))) if slice_off.size > 1 else 0
+        self.unit_regular = int(info.unit_regular) if integer_path else 0
         self.device = torch.device(device)
         t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(self.device)
         self.d_color_ptr, self.d_slice_off, self.d_ell_nbr = t(color_ptr), t(slice_off), t(ell_nbr)
@@ -118,7 +119,7 @@ class DeviceProblem:
     def c_problem(self) -> _lib.DeviceProblem:
         return _lib.DeviceProblem(self.n, self.n_pos, self.n_slices, self.info.n_colors, 1 if self.integer_path else 0,
                                   self.max_field, self.max_width, self.max_class, self.info.has_field,
-                                  self.min_width, self.n_ell,
+                                  self.min_width, self.unit_regular, self.n_ell,
                                   self.d_color_ptr.data_ptr(), self.d_slice_off.data_ptr(), self.d_ell_nbr.data_ptr(),
                                   self.d_ell_w.data_ptr(), self.d_h_pos.data_ptr())
 
@@ -131,7 +132,7 @@ class PtEngine:
 
     def __init__(self, prob: DeviceProblem, betas, *, seed: int = 0, sweeps_per_round: int = 1, instance: int = 0,
                  replicas_per_cta: int = 0, threads_per_cta: int = 0, positions_per_item: int = 0,
-                 timeout_s: float = 10.0, round_sync: int = 0):
+                 timeout_s: float = 10.0, round_sync: int = 0, item_form: int = 0):
         import torch
 
         self.torch = torch
@@ -148,6 +149,7 @@ class PtEngine:
         self.rpc, self.threads, self.timeout_s = int(replicas_per_cta), int(threads_per_cta), float(timeout_s)
         self.ppi = int(positions_per_item)
         self.round_sync = int(round_sync)  # 0 auto, 1 grid barrier, 2 one cluster
+        self.item_form = int(item_form)  # 0 auto, 1 sliced-ELL gather, 2 unit-regular sweep
         dev = prob.device
         L = _lib.load()
         self.d_betas = torch.from_numpy(self.betas).to(dev)
@@ -174,7 +176,7 @@ class PtEngine:
 
     def _args(self, n_rounds: int) -> _lib.RunArgs:
         return _lib.RunArgs(self.R, n_rounds, self.spr, self.round_sync, self.rounds_done, self.seed & 0xFFFFFFFFFFFFFFFF,
-                            self.instance, self.rpc, self.threads, self.ppi, self.d_betas.data_ptr(),
+                            self.instance, self.rpc, self.threads, self.ppi, self.item_form, self.d_betas.data_ptr(),
                             self.d_thr.data_ptr() if self.thr is not None else None, self.timeout_s)
 
     def _state(self, history=None) -> _lib.DeviceState:

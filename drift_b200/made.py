@@ -44,8 +44,10 @@ def _bind():
         L.drift_pt_colsum_bf16.argtypes = [i32, i32, vp, vp, vp]
         L.drift_pt_adam.argtypes = [i32, i32, vp, vp, vp, vp, vp, f32, f32, f32, f32, i32, vp, vp, vp]
         L.drift_pt_made_sample.argtypes = [C.POINTER(MadeNetC), i32, i32, vp, vp, C.c_uint64, C.c_uint32, vp]
+        L.drift_pt_made_sample_suffix.argtypes = [C.POINTER(MadeNetC), i32, i32, vp, vp, C.c_uint64, C.c_uint32, vp]
         for name in ("drift_pt_gemm_bf16", "drift_pt_made_loss", "drift_pt_made_spins_to_bf16",
-                     "drift_pt_transpose_bf16", "drift_pt_colsum_bf16", "drift_pt_adam", "drift_pt_made_sample"):
+                     "drift_pt_transpose_bf16", "drift_pt_colsum_bf16", "drift_pt_adam", "drift_pt_made_sample",
+                     "drift_pt_made_sample_suffix"):
             getattr(L, name).restype = C.c_int
         L._made_bound = True
     return L
@@ -224,6 +226,24 @@ class Made:
         self.check()
         return hist
 
+    def train_async(self, data, *, steps: int, batch: int = 512, lr: float = 1e-3, seed: int = 0):
+        """Enqueue `steps` minibatch Adam steps on the current stream without synchronising the host:
+        minibatches are drawn on the device (uniform with replacement from data [M][n]), and the
+        mean log q of each step's batch is left in a device tensor [steps] (returned). Lets the
+        network train on a side stream while other work (plain PT) runs on another."""
+        torch = self.torch
+        M = data.shape[0]
+        batch = min(batch, M - M % 8) if M >= 8 else M
+        g = torch.Generator(device=self.device).manual_seed(seed)
+        idx = torch.randint(0, M, (steps, batch), device=self.device, generator=g)
+        out = torch.empty(steps, dtype=torch.float32, device=self.device)
+        for k in range(steps):
+            xb = data.index_select(0, idx[k]).contiguous()
+            lq = self.loss_and_grad(xb)
+            self.step(lr)
+            out[k] = lq.mean()
+        return out
+
     def check(self):
         self.torch.cuda.synchronize(self.device)
         if int(self.err.item()):
@@ -239,6 +259,16 @@ class Made:
                                                 seed & 0xFFFFFFFFFFFFFFFF, stream_id & 0xFFFFFFFF, self._stream()),
                    "drift_pt_made_sample")
         return x, lq
+
+    def sample_suffix(self, x, keep: int, seed: int, stream_id: int = 0):
+        """In place on int8 configurations x [count][n]: keep spins 0..keep-1, draw the others from
+        q's conditionals; returns the log q (fp32 [count]) of the results."""
+        lq = self.torch.empty(x.shape[0], dtype=self.torch.float32, device=self.device)
+        net = self.net_c()
+        _lib.check(_bind().drift_pt_made_sample_suffix(C.byref(net), x.shape[0], int(keep), self._p(x), self._p(lq),
+                                                       seed & 0xFFFFFFFFFFFFFFFF, stream_id & 0xFFFFFFFF,
+                                                       self._stream()), "drift_pt_made_sample_suffix")
+        return lq
 
     def logq(self, x):
         """log q of int8 configurations x [count][n] (same arithmetic as sample())."""

@@ -1,9 +1,13 @@
 """Neural-proposal parallel tempering on dense models: plain PT rounds of the dense-coupling engine
-(drift_b200.sk) alternated with whole-configuration proposals from a trained MADE (drift_b200.made)
-at the coldest rungs, each accepted by the exact Metropolis-Hastings test of drift_pt_made_mh. The
-proposals are independent of the current state, so the test uses q(x) / q(x'); energies are exact
-integers, so the stationary distribution of every rung is the same Boltzmann distribution as plain
-PT's, and plain PT remains the fallback between proposals.
+(drift_b200.sk) alternated with proposals from a trained MADE (drift_b200.made) at the coldest rungs,
+each accepted by the exact Metropolis-Hastings test of drift_pt_made_mh.
+
+Two kinds of proposal: independent whole configurations x' ~ q, or (``suffix=m``) conditional ones
+that keep a replica's first n - m spins and redraw the last m from q's conditionals given them. For
+both, the test's ratio is q(x) / q(x') (for the conditional proposal the kept spins' factors of q
+cancel between the forward and the reverse move). Energies are exact integers, so the stationary
+distribution of every rung is the same Boltzmann distribution as plain PT's, and plain PT remains
+the fallback between proposals.
 """
 
 from __future__ import annotations
@@ -53,12 +57,15 @@ class NeuralPT:
 
     def __init__(self, model: SkModel, betas, made: Made, *, seed: int = 0, sweeps_per_round: int = 10,
                  n_cold: int = 8, replicas_per_cta: int = 0, instance: int = 0, device="cuda",
-                 engine: SkEngine | None = None):
+                 engine: SkEngine | None = None, suffix: int | None = None):
         # `engine`: continue an existing plain-PT run (e.g. the one whose samples trained `made`)
         self.eng = engine or SkEngine(model, betas, seed=seed, sweeps_per_round=sweeps_per_round, instance=instance,
                                       replicas_per_cta=replicas_per_cta, device=device)
         self.made = made
         self.n_cold = n_cold
+        if suffix is not None and not 1 <= suffix <= model.n:
+            raise ValueError("suffix must be in [1, n]")
+        self.suffix = suffix  # None: independent proposals; m: redraw the last m spins
         torch = self.torch = self.eng.torch
         R = self.eng.R
         self.prop_tried = torch.zeros(R, dtype=torch.int64, device=self.eng.device)
@@ -73,7 +80,11 @@ class NeuralPT:
     def propose(self, round_index: int):
         eng, made = self.eng, self.made
         R = eng.R
-        xp, lq_p = made.sample(R, seed=eng.seed ^ 0x5EED, stream_id=round_index)
+        if self.suffix is None:
+            xp, lq_p = made.sample(R, seed=eng.seed ^ 0x5EED, stream_id=round_index)
+        else:
+            xp = eng.spins.clone()
+            lq_p = made.sample_suffix(xp, made.n - self.suffix, seed=eng.seed ^ 0x5EED, stream_id=round_index)
         lq_c = made.logq(eng.spins)
         e_p = self.torch.empty(R, dtype=self.torch.int64, device=eng.device)
         P = eng._problem()

@@ -94,6 +94,10 @@ typedef struct DriftPtLayoutInfo {
   int32_t max_field;         /* F = max_i (sum_j |J_ij| + |h_i|) on the integer path        */
   int32_t has_field;         /* 1 if some h_i != 0                                          */
   int32_t min_width;         /* smallest slice width (== max_degree: uniform, e.g. lattices) */
+  int32_t unit_regular;      /* 1 if every spin has max_degree couplings, every coupling is
+                                +1 or -1 and there is no field (MaxCut on regular graphs,
+                                +-J lattices): such problems can run the unit-regular sweep
+                                (item_form 2 of the run args)                               */
 } DriftPtLayoutInfo;
 
 DRIFT_PT_API int drift_pt_layout_query(const DriftPtCsr* csr, DriftPtLayoutInfo* info);
@@ -126,7 +130,8 @@ typedef struct DriftPtDeviceProblem {
   int32_t max_class;         /* size of the largest colour class                            */
   int32_t has_field;         /* 0 if every h_i == 0 (the field is then never read)          */
   int32_t min_width;         /* smallest slice width; the layout's values of max_field,
-                                max_width and min_width must be passed unchanged            */
+                                max_width, min_width and unit_regular must be passed unchanged */
+  int32_t unit_regular;      /* DriftPtLayoutInfo.unit_regular (0 is always allowed)        */
   int64_t n_ell;
   const int32_t* color_ptr;
   const int32_t* slice_off;
@@ -168,6 +173,12 @@ typedef struct DriftPtRunArgs {
   int32_t threads_per_cta;   /* 0 = auto; at most 512                                       */
   int32_t positions_per_item;/* 8, 4 or 1 spins per thread and phase (4 and 1: integer path;
                                 1: coupling table in shared memory); 0 = auto               */
+  int32_t item_form;         /* how an item reads its neighbours: 0 = auto, 1 = the sliced
+                                ELL gather (any problem), 2 = the unit-regular sweep (problems
+                                with unit_regular set, one replica per CTA, 8 positions per
+                                item: neighbour addresses precomputed in shared memory, spins
+                                as 0/1 bytes with a sign-flipped copy, the decision looked up
+                                by (spin, unsatisfied-bond count)). Results do not depend on it. */
   const double* betas;       /* [R] inverse temperature of each rung                        */
   const uint32_t* thresholds;/* [R][F] integer path (from drift_pt_thresholds), else NULL   */
   double timeout_s;          /* bound on any in-kernel wait (0 = 10 s)                      */
@@ -199,13 +210,17 @@ DRIFT_PT_API int drift_pt_run(const DriftPtDeviceProblem* prob, const DriftPtRun
  * The first call on a device looks up the array's device address (cudaGetSymbolAddress) while
  * that device is current; make that first call before any stream capture. All calls in the
  * process share the one array: calls that overlap on the GPU (other streams, other threads) race
- * on it and must be serialised by the caller. A timed-out in-kernel wait is not reported by this
- * entry point (drift_pt_check needs the workspace address); use drift_pt_run where that matters.
- * No counterpart in the reference: its engine allocates all device memory itself
- * (cuda/ising_pt.cu:180-195) and has no allocation-free mode. */
+ * on it and must be serialised by the caller. Call drift_pt_noalloc_check() to learn whether a
+ * bounded in-kernel wait timed out. No counterpart in the reference. */
 #define DRIFT_PT_NOALLOC_MAX_REPLICAS 4096
 DRIFT_PT_API int drift_pt_run_noalloc(const DriftPtDeviceProblem* prob, const DriftPtRunArgs* args,
                                       DriftPtDeviceState* state, void* stream);
+
+/* drift_pt_check for drift_pt_run_noalloc: synchronises the stream and returns DRIFT_PT_ETIMEOUT
+ * if the built-in scratch array's error flag is set (the last run's bounded wait gave up and its
+ * state is incomplete). Reads the flag with a synchronous copy from the array; allocates nothing.
+ * No counterpart in the reference. */
+DRIFT_PT_API int drift_pt_noalloc_check(void* stream);
 
 /* Synchronises the stream and returns DRIFT_PT_ETIMEOUT if the workspace's error flag is set. */
 DRIFT_PT_API int drift_pt_check(void* workspace, void* stream);
@@ -586,7 +601,7 @@ typedef struct DriftPtMadeNet { /* device arrays */
 /* mode 0: draw count configurations x [count][n] (+-1) from q with Philox(i, sample, stream_id,
  * 8 << 24; seed) and return log q of each; mode 1: log q of the given x. Both walk the spins in
  * order and accumulate every sum in one fixed order, so the log q of a drawn x equals its
- * mode-1 value exactly. */
+ * mode-1 value exactly. No counterpart in the reference (it has no learned component). */
 DRIFT_PT_API int drift_pt_made_sample(const DriftPtMadeNet* net, int32_t count, int32_t mode, int8_t* x,
                                       float* logq, uint64_t seed, uint32_t stream_id, void* stream);
 
@@ -596,6 +611,14 @@ DRIFT_PT_API int drift_pt_made_sample(const DriftPtMadeNet* net, int32_t count, 
  * energies (units 2^-(shift+1)) and the fp32 log q values; uniform from
  * Philox(slot, round lo, round hi, 9 << 24 | instance; seed). Counts per rung in prop_tried /
  * prop_accepted [R]; an accepted proposal below the slot's best also becomes its best. */
+/* Conditional proposals: for each of the count configurations in x [count][n], keep spins
+ * 0 .. keep-1 and draw spins keep .. n-1 from q's conditionals given them (uniforms as in mode 0);
+ * x is overwritten with the result and logq receives its full log q, bit-identical to mode 1 on the
+ * result. A Metropolis-Hastings test with this proposal uses q(x) / q(x') exactly like an
+ * independent draw, because the kept spins' factors of q cancel. No counterpart in the reference. */
+DRIFT_PT_API int drift_pt_made_sample_suffix(const DriftPtMadeNet* net, int32_t count, int32_t keep, int8_t* x,
+                                             float* logq, uint64_t seed, uint32_t stream_id, void* stream);
+
 DRIFT_PT_API int drift_pt_made_mh(const DriftPtSkProblem* problem, const DriftPtSkRunArgs* args, DriftPtSkState* state,
                                   const int8_t* proposals, const int64_t* prop_energy, const float* logq_prop,
                                   const float* logq_cur, const uint8_t* active, int64_t* prop_tried,

@@ -160,6 +160,26 @@ def test_batch_rounds_replayed_from_a_cuda_graph():
             assert np.array_equal(a[key], b[key]), f"instance {k}: {key}"
 
 
+def test_whole_job_graph_replays_the_job():
+    """BatchEngine.capture_job: initialisation and every round in one CUDA graph; each replay is the
+    eager job bit for bit (one launch, or launches of 3 rounds)."""
+    models, ladders = int_batch()
+    rounds, spr, seed = 8, 2, 17
+    _, eager = run_batch(models, ladders, rounds, spr, seed)
+    for launch_rounds in (0, 3):
+        bp = BatchProblem([HostProblem.from_model(m) for m in models], ladders)
+        eng = BatchEngine(bp, seed=seed, sweeps_per_round=spr)
+        job = eng.capture_job(rounds, launch_rounds)
+        assert job.launches == (1 if launch_rounds == 0 else 3)
+        for _ in range(2):
+            job.replay()
+            eng.check()
+            for k in range(len(models)):
+                a, b = eager.fetch(k), eng.fetch(k)
+                for key in KEYS:
+                    assert np.array_equal(a[key], b[key]), f"instance {k}: {key}"
+
+
 def test_autotune_picks_a_shape_and_keeps_results():
     models, ladders = int_batch()
     rounds, spr, seed = 5, 2, 8

@@ -125,6 +125,57 @@ def test_sampler_draws_from_q():
     assert chi2 < dof + 6 * np.sqrt(2 * dof), (chi2, dof)
 
 
+def test_suffix_sampler_keeps_the_prefix_and_its_logq_is_one_function():
+    import torch
+
+    from drift_b200.made import Made
+
+    n, h = 64, 128
+    made = Made(n, (h, h), seed=7)
+    for k in range(3):
+        made.b[k].normal_(0.0, 0.3)
+    x0, _ = made.sample(40, seed=5, stream_id=1)
+    x = x0.clone()
+    lq = made.sample_suffix(x, 40, seed=11, stream_id=2)
+    assert torch.equal(x[:, :40], x0[:, :40])
+    assert not torch.equal(x[:, 40:], x0[:, 40:])
+    assert torch.equal(lq, made.logq(x))  # bit for bit, as for whole draws
+    y = x0.clone()
+    assert torch.equal(made.sample_suffix(y, n, seed=11, stream_id=2), made.logq(x0)) and torch.equal(y, x0)
+
+
+def test_suffix_sampler_draws_from_the_conditionals():
+    """Chi-square of 100,000 redraws of the last 3 spins of an n = 8 network given fixed first 5,
+    against the exact conditional q(x_5, x_6, x_7 | x_0..x_4)."""
+    import torch
+
+    from drift_b200.made import Made
+
+    n, keep = 8, 5
+    made = Made(n, (16, 16), seed=2)
+    for k in range(3):
+        made.b[k].normal_(0.0, 0.8)
+    W, b = made.weights_host()
+    xs, lq = made_ref.all_logq(W, b, n)
+    prefix = np.array([1, -1, -1, 1, 1], np.int8)
+    sel = np.all(xs[:, :keep] == prefix, axis=1)
+    p = np.exp(lq[sel])
+    p /= p.sum()
+    N = 100_000
+    x = torch.from_numpy(np.tile(np.concatenate([prefix, np.ones(n - keep, np.int8)]), (N, 1))).cuda()
+    made.sample_suffix(x, keep, seed=4)
+    xh = x.cpu().numpy()
+    assert np.all(xh[:, :keep] == prefix)
+    w = 1 << np.arange(n - keep - 1, -1, -1)
+    codes = ((xh[:, keep:] > 0).astype(np.int64) * w).sum(1)
+    ref_codes = ((xs[sel][:, keep:] > 0).astype(np.int64) * w).sum(1)
+    counts = np.bincount(codes, minlength=1 << (n - keep))[ref_codes]
+    expected = p * N
+    chi2 = (((counts - expected) ** 2) / expected).sum()
+    dof = len(p) - 1
+    assert chi2 < dof + 6 * np.sqrt(2 * dof), (chi2, dof)
+
+
 def test_training_raises_the_likelihood_of_the_data():
     import torch
 
@@ -143,9 +194,10 @@ def test_training_raises_the_likelihood_of_the_data():
     assert hist[-1] > -9.0, hist
 
 
-@pytest.mark.parametrize("trained", [False, True])
-def test_neural_pt_is_stationary_at_the_boltzmann_distribution(trained):
-    """SK n = 16: per-rung mean energy of neural-proposal PT vs exact enumeration."""
+@pytest.mark.parametrize("trained,suffix", [(False, None), (True, None), (True, 6)])
+def test_neural_pt_is_stationary_at_the_boltzmann_distribution(trained, suffix):
+    """SK n = 16: per-rung mean energy of neural-proposal PT vs exact enumeration, with independent
+    proposals and with conditional ones that redraw the last 6 spins."""
     from drift_b200.instances import sk_model
     from drift_b200.made import Made
     from drift_b200.neural import NeuralPT, collect_cold_samples
@@ -161,7 +213,7 @@ def test_neural_pt_is_stationary_at_the_boltzmann_distribution(trained):
         data = collect_cold_samples(pre, 4096, n_cold=2)
         made.train(data, epochs=10, batch=256, lr=3e-3)
     ex = oracle.exact(sk.Jq * 2.0 ** -sk.shift, sk.hq * 2.0 ** -sk.shift, betas)
-    npt = NeuralPT(sk, betas, made, seed=4, sweeps_per_round=1, n_cold=4)
+    npt = NeuralPT(sk, betas, made, seed=4, sweeps_per_round=1, n_cold=4, suffix=suffix)
     npt.init()
     npt.run(50)
     es = []

@@ -62,3 +62,76 @@ def test_multispin_resume_and_large_lattice_energies():
     st = e.fetch()
     assert np.array_equal(big.energy(st["spins"][:8]).astype(np.int64), st["energy"][:8])
     assert np.all(st["best_energy"] <= st["energy"])
+
+
+def _ms_series(lat, betas, rounds, spr, seed):
+    """Per-round rung energies and |m| of the multispin engine (one launch per round)."""
+    import torch
+
+    eng = MsEngine(lat, betas, seed=seed, sweeps_per_round=spr)
+    eng.init()
+    R = len(betas)
+    E = torch.zeros((rounds, R), dtype=torch.int64, device="cuda")
+    words = torch.zeros((rounds, eng.W * lat.n), dtype=torch.int32, device="cuda")
+    slots = torch.zeros((rounds, R), dtype=torch.int64, device="cuda")
+    for t in range(rounds):
+        eng.run(1)
+        sor = eng.slot_of_rung.long()
+        E[t] = eng.energy[sor]
+        words[t] = eng.words
+        slots[t] = sor
+    eng.check()
+    w = words.cpu().numpy().view(np.uint32).reshape(rounds, eng.W, lat.n)
+    bits = (w[:, :, None, :] >> np.arange(32, dtype=np.uint32)[None, None, :, None]) & 1
+    m = np.abs((1 - 2 * bits.astype(np.float64)).reshape(rounds, R, lat.n).mean(axis=2))
+    absm = np.take_along_axis(m, slots.cpu().numpy(), axis=1)
+    return E.cpu().numpy().astype(np.float64), absm
+
+
+def test_multispin_engine_samples_the_boltzmann_distribution():
+    """The kernel's chain on a 2-D +-J L = 4 lattice: per-rung mean energy and |m| within 3 standard
+    errors (blocked; floored by the exact variance over the samples) of exact enumeration
+    (drift/solvers/exact.py:20-49, oracle/exact.c)."""
+    from drift_b200.observables import blocked
+    from test_multispin import dense_couplings
+
+    lat = Lattice.edwards_anderson(2, 4, 3)
+    betas = ladder(32, 0.2, 3.0)
+    ex = oracle.exact(dense_couplings(lat), np.zeros(lat.n), betas)
+    E, M = _ms_series(lat, betas, 4000, 2, 9)
+    n_kept = len(E) - int(len(E) * 0.1)
+    for x, mean, mean2 in ((E, ex.mean_e, ex.mean_e2), (M, ex.mean_absm, ex.mean_m2)):
+        mx, sx = blocked(x)
+        floor = np.sqrt(np.maximum(mean2 - mean ** 2, 0.0) / n_kept)
+        assert np.all(np.abs(mx - mean) <= 3.0 * np.maximum(sx, floor) + 1e-9), (mx, mean, sx)
+
+
+@pytest.mark.parametrize("item_form", [1, 2])
+def test_multispin_engine_agrees_with_the_int8_engine(item_form):
+    """3-D +-J L = 4 (64 spins, beyond exact enumeration): the bit-packed chain and the int8 sparse
+    engine (sliced-ELL gather or unit-regular form) have the same per-rung mean energies within 3
+    combined standard errors (blocked)."""
+    import torch
+
+    from drift_b200.engine import DeviceProblem, HostProblem, PtEngine
+    from drift_b200.instances import ea_3d
+    from drift_b200.observables import blocked
+
+    lat = Lattice.edwards_anderson(3, 4, 8)
+    model = ea_3d(4, 8)
+    s = np.random.default_rng(1).choice([-1.0, 1.0], size=(4, lat.n))
+    assert np.allclose(lat.energy(s), model.energy_batch(s))  # the same couplings
+    betas = ladder(32, 0.2, 2.0)
+    rounds, spr = 4000, 2
+    E_ms, _ = _ms_series(lat, betas, rounds, spr, 21)
+    eng = PtEngine(DeviceProblem(HostProblem.from_model(model)), betas, seed=22, sweeps_per_round=spr,
+                   item_form=item_form)
+    eng.init()
+    E = torch.zeros((rounds, len(betas)), dtype=torch.int64, device="cuda")
+    for t in range(rounds):
+        eng.run(1)
+        E[t] = eng.energy[eng.slot_of_rung.long()]
+    eng.check()
+    m1, s1 = blocked(E_ms)
+    m2, s2 = blocked(E.cpu().numpy().astype(np.float64))
+    assert np.all(np.abs(m1 - m2) <= 3.0 * np.sqrt(s1 ** 2 + s2 ** 2) + 1e-9), (m1, m2, s1, s2)

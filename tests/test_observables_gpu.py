@@ -45,3 +45,25 @@ def test_engine_observables_match_exact_and_reference_cpu_pt():
         mr, sr = blocked(ref[k])
         assert np.all(np.abs(mo - mr) <= 3.0 * np.sqrt(so ** 2 + sr ** 2) + 1e-9), (k, mo, mr, so, sr)
     assert a["energy"].min() >= ex.e_min - 1e-9
+
+
+def test_engine_matches_the_reference_cpu_pt_on_c1():
+    """C1 (2-D +-J L = 16, 24 rungs, T 1/3..10, one sweep per round): 16 independent ladders of the
+    engine, each after the same burn-in, against 16 of the reference CPU PT (the fixture of
+    tests/test_c1_observables.py): per-rung mean energy, |m| and overlap q^2 within 3 combined
+    standard errors across runs."""
+    from drift_b200.engine import DeviceProblem, PtEngine
+    from test_c1_observables import assert_agrees_with_reference, c1_setup, summarise
+
+    fx, hp, betas = c1_setup()
+    prob = DeviceProblem(hp)
+    E_runs, M_runs, S_runs = [], [], []
+    for k in range(fx["runs"]):
+        eng = PtEngine(prob, betas, seed=700 + k, sweeps_per_round=1)
+        eng.init()
+        eng.run(fx["burn_in"])
+        run = record(eng, fx["rounds"], spins=True)
+        E_runs.append(run["energy"])
+        M_runs.append(run["absm"])
+        S_runs.append(run["spins"])
+    assert_agrees_with_reference(summarise(E_runs, M_runs, S_runs), fx)

@@ -20,7 +20,7 @@ from conftest import cuda_ready, dense_from_edges
 from drift_b200 import _lib
 from drift_b200.engine import DeviceProblem, HostProblem, PtEngine, geometric_betas
 from drift_b200.gpu import parallel_tempering_gpu
-from drift_b200.instances import (ea_2d, er_gaussian, gnp_pm, maxcut_3regular, maxcut_ising, pm_spin_glass,
+from drift_b200.instances import (ea_2d, ea_3d, er_gaussian, gnp_pm, maxcut_3regular, maxcut_ising, pm_spin_glass,
                                   random_graph, sk_model)
 
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not cuda_ready(), reason="needs CUDA and libdrift_pt.so")]
@@ -32,13 +32,13 @@ def oracle_problem(hp: HostProblem, integer_path: bool):
 
 
 def run_engine(model, betas, rounds, spr, seed, *, rpc=0, threads=0, ppi=0, instance=0, chunks=None,
-               integer_path=None, round_sync=0):
+               integer_path=None, round_sync=0, item_form=0):
     import torch
 
     hp = HostProblem.from_model(model)
     prob = DeviceProblem(hp, integer_path=integer_path)
     eng = PtEngine(prob, betas, seed=seed, sweeps_per_round=spr, instance=instance, replicas_per_cta=rpc,
-                   threads_per_cta=threads, positions_per_item=ppi, round_sync=round_sync)
+                   threads_per_cta=threads, positions_per_item=ppi, round_sync=round_sync, item_form=item_form)
     eng.init()
     hist = torch.zeros(max(rounds, 1), dtype=torch.float64, device="cuda")
     done = 0
@@ -116,24 +116,32 @@ def test_edge_cases_match_oracle_bit_exact(name):
     assert_bit_exact(st, ost, hist, rounds)
 
 
+@pytest.mark.parametrize("item_form", [0, 1])
 @pytest.mark.parametrize("name", list(CASES))
-def test_engine_matches_oracle_bit_exact(name):
+def test_engine_matches_oracle_bit_exact(name, item_form):
+    """item_form 0 lets the engine choose (the unit-regular form for C1 and C2), 1 forces the
+    sliced-ELL gather."""
     make, R, (tmin, tmax), rounds, spr, seed = CASES[name]
     model = make()
     betas = geometric_betas(R, tmin, tmax)
-    hp, prob, eng, st, hist = run_engine(model, betas, rounds, spr, seed)
+    hp, prob, eng, st, hist = run_engine(model, betas, rounds, spr, seed, item_form=item_form)
     ost = oracle.pt_run(oracle_problem(hp, prob.integer_path), betas, n_rounds=rounds, sweeps_per_round=spr,
                         seed=seed, thr=eng.thr)
     assert_bit_exact(st, ost, hist, rounds)
 
 
-@pytest.mark.parametrize("rpc,threads,ppi", [(1, 64, 8), (1, 512, 8), (2, 256, 8), (8, 512, 8), (64, 512, 8),
-                                              (1, 0, 4), (1, 96, 4), (4, 512, 4), (64, 512, 4), (16, 0, 0)])
-def test_results_do_not_depend_on_launch_shape(rpc, threads, ppi):
+@pytest.mark.parametrize("rpc,threads,ppi,form", [(1, 64, 8, 1), (1, 512, 8, 1), (2, 256, 8, 1), (8, 512, 8, 1),
+                                                   (64, 512, 8, 1), (1, 0, 4, 1), (1, 96, 4, 1), (4, 512, 4, 1),
+                                                   (64, 512, 4, 1), (16, 0, 0, 0), (1, 0, 0, 2), (1, 0, 2, 2),
+                                                   (1, 832, 2, 2), (1, 0, 4, 2), (1, 1024, 4, 2)])
+def test_results_do_not_depend_on_launch_shape(rpc, threads, ppi, form):
+    """Form 1 is the sliced-ELL gather, form 2 the unit-regular form (2 or 4 positions per item, the
+    CTA as narrow as the largest class allows or as wide as the form allows)."""
     model = maxcut_3regular(2048, 5)
     R, rounds, spr, seed = 64, 10, 2, 11
     betas = geometric_betas(R, 0.25, 5.0)
-    hp, prob, eng, st, hist = run_engine(model, betas, rounds, spr, seed, rpc=rpc, threads=threads, ppi=ppi)
+    hp, prob, eng, st, hist = run_engine(model, betas, rounds, spr, seed, rpc=rpc, threads=threads, ppi=ppi,
+                                         item_form=form)
     ost = oracle.pt_run(oracle_problem(hp, True), betas, n_rounds=rounds, sweeps_per_round=spr, seed=seed, thr=eng.thr)
     assert_bit_exact(st, ost, hist, rounds)
 
@@ -184,6 +192,68 @@ def test_one_position_per_item_matches_oracle_bit_exact(name, round_sync):
     ost = oracle.pt_run(oracle_problem(hp, True), betas, n_rounds=rounds, sweeps_per_round=spr, seed=seed,
                         thr=eng.thr)
     assert_bit_exact(st, ost, hist, rounds)
+
+
+def _ring_pm(n, seed):
+    """A ring of n spins with +-1 couplings (every spin has 2)."""
+    from drift_b200.ising import SparseIsingModel
+
+    rng = np.random.default_rng(seed)
+    i = np.arange(n)
+    return SparseIsingModel(n, i, (i + 1) % n, rng.choice([-1.0, 1.0], size=n))
+
+
+UNIT_CASES = {
+    # name: (model factory, R, T range, rounds, sweeps_per_round, seed, round_sync)
+    "ea2d_L16_R24_grid": (lambda: ea_2d(16, 1), 24, (1 / 3.0, 10.0), 400, 1, 1, 1),
+    "ea2d_L16_R16_cluster": (lambda: ea_2d(16, 3), 16, (1 / 3.0, 10.0), 400, 1, 2, 2),
+    "ea2d_L5_ragged_R7": (lambda: ea_2d(5, 2), 7, (0.2, 5.0), 80, 3, 7, 0),
+    "ea3d_L6_W6_R20": (lambda: ea_3d(6, 4), 20, (0.2, 5.0), 60, 2, 3, 1),
+    "ea3d_L4_W6_R12_cluster": (lambda: ea_3d(4, 5), 12, (0.2, 5.0), 60, 2, 4, 2),
+    "ring_300_W2_R10": (lambda: _ring_pm(300, 6), 10, (0.2, 5.0), 80, 2, 5, 0),
+    "maxcut_3reg_4096_R64_C2": (lambda: maxcut_3regular(4096, 2), 64, (0.25, 5.0), 25, 4, 7, 0),
+    "maxcut_3reg_2048_R16_cluster": (lambda: maxcut_3regular(2048, 5), 16, (0.25, 5.0), 20, 2, 5, 2),
+    "one_replica": (lambda: maxcut_3regular(512, 3), 1, (0.2, 5.0), 40, 2, 8, 0),
+    "two_replicas": (lambda: maxcut_3regular(512, 3), 2, (0.2, 5.0), 40, 2, 9, 0),
+    "maxcut_3reg_8192_R8_four_per_item": (lambda: maxcut_3regular(8192, 4), 8, (0.25, 5.0), 6, 2, 10, 1),
+}
+
+
+@pytest.mark.parametrize("name", list(UNIT_CASES))
+def test_unit_regular_form_matches_oracle_bit_exact(name):
+    """The unit-regular form (neighbour addresses and a (spin, count) decision table in shared
+    memory) runs the oracle's chain bit for bit: lattices in 2-D and 3-D, a ring, MaxCut on 3-regular
+    graphs, padding positions (25 spins in 256 positions), one and two replicas, grid and cluster
+    round ends."""
+    make, R, (tmin, tmax), rounds, spr, seed, sync = UNIT_CASES[name]
+    model = make()
+    betas = geometric_betas(R, tmin, tmax)
+    hp, prob, eng, st, hist = run_engine(model, betas, rounds, spr, seed, round_sync=sync, item_form=2)
+    assert prob.unit_regular
+    ost = oracle.pt_run(oracle_problem(hp, True), betas, n_rounds=rounds, sweeps_per_round=spr, seed=seed,
+                        thr=eng.thr)
+    assert_bit_exact(st, ost, hist, rounds)
+
+
+def test_unit_regular_form_resumes_and_checks_its_energy():
+    model = maxcut_3regular(1024, 8)
+    betas = geometric_betas(32, 0.25, 5.0)
+    chunks = [5, 1, 7]
+    hp, prob, eng, st, hist = run_engine(model, betas, sum(chunks), 3, 13, chunks=chunks, item_form=2)
+    ost = oracle.pt_run(oracle_problem(hp, True), betas, n_rounds=sum(chunks), sweeps_per_round=3, seed=13,
+                        thr=eng.thr)
+    assert_bit_exact(st, ost, hist, sum(chunks))
+    assert np.array_equal(eng.energy_fp64(), st["energy_fixed"].astype(np.float64))
+
+
+def test_unit_regular_form_refuses_other_problems():
+    betas = geometric_betas(8, 0.25, 5.0)
+    with pytest.raises(_lib.EngineError, match="unit-regular"):
+        run_engine(gnp_pm(64, 0.1, 2), betas, 2, 1, 0, item_form=2)  # irregular degrees
+    with pytest.raises(_lib.EngineError, match="unit-regular"):
+        run_engine(maxcut_3regular(512, 1), betas, 2, 1, 0, rpc=2, item_form=2)  # two replicas per CTA
+    with pytest.raises(_lib.EngineError, match="item_form 2"):
+        run_engine(maxcut_3regular(2048, 1), betas, 2, 1, 0, threads=64, item_form=2)  # one item per thread
 
 
 def test_cluster_form_refuses_a_ladder_that_does_not_fit():
