@@ -17,7 +17,8 @@ OK, EINVAL, ECUDA, ETIMEOUT, ENOMEM, EUNSUPPORTED = 0, 1, 2, 3, 4, 5
 # Every symbol include/drift_pt.h declares.
 EXPORTED = (
     "drift_pt_version", "drift_pt_last_error", "drift_pt_greedy_coloring", "drift_pt_color_order",
-    "drift_pt_layout_query", "drift_pt_layout_fill", "drift_pt_thresholds", "drift_pt_workspace_bytes",
+    "drift_pt_layout_query", "drift_pt_layout_fill", "drift_pt_unit_placement", "drift_pt_thresholds",
+    "drift_pt_workspace_bytes",
     "drift_pt_init", "drift_pt_run", "drift_pt_check", "drift_pt_energy_fp64", "drift_pt_solve",
     "drift_pt_run_noalloc", "drift_pt_noalloc_check", "drift_pt_batch_items", "drift_pt_batch_init", "drift_pt_batch_workspace_bytes",
     "drift_pt_batch_run", "drift_pt_ms_workspace_bytes", "drift_pt_ms_init", "drift_pt_ms_run",
@@ -55,7 +56,8 @@ class DeviceProblem(C.Structure):
                 ("integer_path", C.c_int32), ("max_field", C.c_int32), ("max_width", C.c_int32),
                 ("max_class", C.c_int32), ("has_field", C.c_int32), ("min_width", C.c_int32),
                 ("unit_regular", C.c_int32), ("n_ell", C.c_int64),
-                ("color_ptr", vp), ("slice_off", vp), ("ell_nbr", vp), ("ell_w", vp), ("h_pos", vp)]
+                ("color_ptr", vp), ("slice_off", vp), ("ell_nbr", vp), ("ell_w", vp), ("h_pos", vp),
+                ("unit_place", vp)]
 
 
 class DeviceState(C.Structure):
@@ -124,6 +126,7 @@ def load():
     L.drift_pt_layout_query.argtypes = [C.POINTER(Csr), C.POINTER(LayoutInfo)]
     L.drift_pt_layout_fill.argtypes = [C.POINTER(Csr), C.c_int32, C.POINTER(Layout)]
     L.drift_pt_thresholds.argtypes = [C.c_int32, vp, C.c_int32, vp]
+    L.drift_pt_unit_placement.argtypes = [C.POINTER(Csr), C.c_int32, vp]
     L.drift_pt_workspace_bytes.argtypes = [C.c_int32, C.POINTER(C.c_size_t)]
     L.drift_pt_init.argtypes = [C.POINTER(DeviceProblem), C.POINTER(RunArgs), C.POINTER(DeviceState), vp]
     L.drift_pt_run.argtypes = [C.POINTER(DeviceProblem), C.POINTER(RunArgs), C.POINTER(DeviceState), vp,

@@ -20,7 +20,7 @@ ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 SOURCES = ["dpt_host.cpp", "dpt_kernels.cu", "dpt_capi.cu", "dpt_noalloc.cu", "dpt_batched.cu", "dpt_multispin.cu",
            "dpt_sk_host.cpp", "dpt_sk.cu", "dpt_gemm.cu", "dpt_made.cu", "dpt_gms_host.cpp", "dpt_gms.cu",
-           "dpt_batch_mh.cu", "dpt_batch_host.cpp"]
+           "dpt_batch_mh.cu", "dpt_batch_host.cpp", "dpt_unit_host.cpp"]
 
 
 def nvcc() -> str:

@@ -116,6 +116,7 @@ PtKernelArgs make_args(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, D
   a.ell_nbr = p->ell_nbr;
   a.ell_w = p->ell_w;
   a.h_pos = p->h_pos;
+  a.unit_place = p->unit_place;
   a.R = r->n_replicas;
   a.spr = r->sweeps_per_round;
   a.n_rounds = r->n_rounds;
@@ -284,7 +285,7 @@ int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPl
     const int W = p->max_width;
     // items of the largest colour class: a class of m positions touches at most (m + 14) / 8 groups
     auto items_of = [&](int P_) { return ((p->max_class + 14) / kGroup) * (kGroup / P_); };
-    const int PU = P_user ? P_user : (items_of(2) <= unit_max_threads(2) ? 2 : 4);
+    const int PU = P_user ? P_user : unit_auto_positions(p->max_class);
     auto total_u = [&](int threads_, bool cl) {
       return smem_layout(p->n_pos, 1, R, p->max_field, p->n_colors, p->n_slices, p->n_ell, true, true, threads_, cl,
                          W, PU)
@@ -607,6 +608,13 @@ extern "C" int drift_pt_solve(const DriftPtCsr* csr, const DriftPtSolveArgs* arg
   if (rc) return rc;
   int max_class = 1;
   for (int c = 0; c < info.n_colors; ++c) max_class = std::max(max_class, color_ptr[c + 1] - color_ptr[c]);
+  // the unit-regular form's storage order of spin bytes
+  std::vector<uint16_t> place;
+  if (ip && info.unit_regular) {
+    place.resize((size_t)info.n_pos / 4);
+    rc = drift_pt_unit_placement(csr, 0, place.data());
+    if (rc) return rc;
+  }
   // ---- device arena ----
   size_t ws_bytes = 0;
   drift_pt_workspace_bytes(R, &ws_bytes);
@@ -617,7 +625,8 @@ extern "C" int drift_pt_solve(const DriftPtCsr* csr, const DriftPtSolveArgs* arg
                o_sp = bump(off, (size_t)R * info.n_pos), o_bsp = bump(off, (size_t)R * info.n_pos),
                o_e = bump(off, (size_t)R * 8), o_be = bump(off, (size_t)R * 8), o_rs = bump(off, (size_t)R * 4),
                o_sr = bump(off, (size_t)R * 4), o_tr = bump(off, (size_t)R * 8), o_ac = bump(off, (size_t)R * 8),
-               o_bh = bump(off, (size_t)std::max(1, args->n_rounds) * 8), o_ws = bump(off, ws_bytes);
+               o_bh = bump(off, (size_t)std::max(1, args->n_rounds) * 8), o_ws = bump(off, ws_bytes),
+               o_pl = bump(off, place.size() * 2);
   DeviceArena arena;
   cudaError_t e = cudaMalloc(&arena.base, off);
   if (e != cudaSuccess) {
@@ -632,7 +641,8 @@ extern "C" int drift_pt_solve(const DriftPtCsr* csr, const DriftPtSolveArgs* arg
       (e = h2d(o_so, slice_off.data(), slice_off.size() * 4)) != cudaSuccess ||
       (e = h2d(o_nb, ell_nbr.data(), ell_nbr.size() * 4)) != cudaSuccess ||
       (e = h2d(o_w, ell_w.data(), ell_w.size())) != cudaSuccess || (e = h2d(o_h, h_pos.data(), h_pos.size())) != cudaSuccess ||
-      (e = h2d(o_beta, betas.data(), (size_t)R * 8)) != cudaSuccess || (e = h2d(o_thr, thr.data(), thr.size() * 4)) != cudaSuccess)
+      (e = h2d(o_beta, betas.data(), (size_t)R * 8)) != cudaSuccess || (e = h2d(o_thr, thr.data(), thr.size() * 4)) != cudaSuccess ||
+      (e = h2d(o_pl, place.data(), place.size() * 2)) != cudaSuccess)
     return cuda_fail(e, "solve: upload");
   DriftPtDeviceProblem prob;
   std::memset(&prob, 0, sizeof prob);
@@ -653,6 +663,7 @@ extern "C" int drift_pt_solve(const DriftPtCsr* csr, const DriftPtSolveArgs* arg
   prob.ell_nbr = reinterpret_cast<const int32_t*>(d + o_nb);
   prob.ell_w = d + o_w;
   prob.h_pos = d + o_h;
+  prob.unit_place = place.empty() ? nullptr : reinterpret_cast<const uint16_t*>(d + o_pl);
   DriftPtDeviceState st;
   st.spins = reinterpret_cast<int8_t*>(d + o_sp);
   st.best_spins = reinterpret_cast<int8_t*>(d + o_bsp);

@@ -127,18 +127,18 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
 
   // ---- stage state and tables ----
   if constexpr (kUnit) {
+    // the storage word of each 4-position word (identity without a placement), then the spins:
     // +1 -> 0 and -1 -> 1 (the sign bit of each byte), the flipped copy, and 16 zero bytes
-    const int chunks = n_pos / 16;
-    const uint4* src = reinterpret_cast<const uint4*>(a.spins + (size_t)s0 * n_pos);
-    for (int i = tid; i < nloc * chunks; i += B) {
-      const int sl = i / chunks, c = i - sl * chunks;
-      const uint4 v = src[i];
-      const uint4 b = make_uint4((v.x >> 7) & 0x01010101u, (v.y >> 7) & 0x01010101u, (v.z >> 7) & 0x01010101u,
-                                 (v.w >> 7) & 0x01010101u);
-      unsigned char* base = smem + L.spins + (size_t)sl * sp_stride;
-      *reinterpret_cast<uint4*>(base + 16 * c) = b;
-      *reinterpret_cast<uint4*>(base + n_pos + 16 * c) =
-          make_uint4(b.x ^ 0x01010101u, b.y ^ 0x01010101u, b.z ^ 0x01010101u, b.w ^ 0x01010101u);
+    uint16_t* place = reinterpret_cast<uint16_t*>(smem + L.h);
+    for (int u = tid; u < n_pos / 4; u += B) place[u] = a.unit_place ? a.unit_place[u] : (uint16_t)u;
+    __syncthreads();
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(a.spins + (size_t)s0 * n_pos);
+    for (int i = tid; i < nloc * (n_pos / 4); i += B) {
+      const int sl = i / (n_pos / 4), u = i - sl * (n_pos / 4);
+      const uint32_t b = (src[i] >> 7) & 0x01010101u;
+      unsigned char* base = smem + L.spins + (size_t)sl * sp_stride + 4 * (size_t)place[u];
+      *reinterpret_cast<uint32_t*>(base) = b;
+      *reinterpret_cast<uint32_t*>(base + n_pos) = b ^ 0x01010101u;
     }
     for (int i = tid; i < nloc; i += B)
       *reinterpret_cast<uint4*>(smem + L.spins + (size_t)i * sp_stride + 2 * n_pos) = make_uint4(0, 0, 0, 0);
@@ -189,6 +189,7 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
   T.wf = static_cast<const float*>(a.ell_w);
   T.h = a.h_pos;
   if constexpr (kUnit) {
+    const uint16_t* place = reinterpret_cast<const uint16_t*>(smem + L.h);
     // neighbour-address rows, one per item of P positions: entry i W + d is the 16-bit address of
     // the byte neighbour d of position P item + i contributes, in the slot's b array (+1 coupling)
     // or b ^ 1 array (-1 coupling); padding entries (weight 0, on padding positions only) point at
@@ -203,8 +204,9 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
       const int S = p >> 8, lane = (p >> 3) & 31, q = p & 7;
       const long long e = (long long)(S * kUnitW + d) * kSlicePositions + q * 32 + lane;
       const int wt = w8[e];
+      const uint32_t nq = (uint32_t)a.ell_nbr[e];
       const uint32_t at = wt == 0 ? base + 2u * (uint32_t)n_pos
-                                  : base + (wt < 0 ? (uint32_t)n_pos : 0u) + (uint32_t)a.ell_nbr[e];
+                                  : base + (wt < 0 ? (uint32_t)n_pos : 0u) + 4u * place[nq >> 2] + (nq & 3u);
       desc[(size_t)(p / P) * (RB / 2) + (p % P) * kUnitW + d] = (uint16_t)at;
     }
     // the Philox blocks of the launch's first sweep (the items compute each later sweep's ahead)
@@ -260,7 +262,8 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
   const int k = a.n_colors;
   const uint32_t c_sweep = ctr3(kTagSweep, a.inst), c_second = ctr3(kTagSecond, a.inst);
   // Unit-regular form: each thread's work in each colour phase is the same every sweep, so it is
-  // fixed here once: item lt of the class (item index | in-class mask << 16 | 1 << 31, or 0) and the
+  // fixed here once: item lt of the class (item index | in-class mask << 14 | storage word of its
+  // first position << 18 | 1 << 31, or 0: n_pos <= 32760 keeps the fields within 14 and 13 bits) and the
   // group whose next-sweep Philox block the thread computes (group + 1, or 0): the groups whose first
   // position lies in the class, taken by the CTA's last threads. (Moving all blocks to the phases
   // with the most idle threads instead measured slower on MaxCut N = 4096: the small phases became
@@ -277,7 +280,8 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
       if (lt < (ghi - glo) * NB) {
         const uint32_t item = (uint32_t)(glo * NB + lt);
         const uint32_t msk = range_mask<P>((int)item * P, lo, hi);
-        s_item[c] = msk ? (item | (msk << 16) | 0x80000000u) : 0u;
+        const uint32_t word = reinterpret_cast<const uint16_t*>(smem + L.h)[(item * P) >> 2];
+        s_item[c] = msk ? (item | (msk << 14) | (word << 18) | 0x80000000u) : 0u;
       }
       const int gp = (lo + 7) / kGroup + (tps - 1 - lt);
       if (gp < (hi + 7) / kGroup) s_px[c] = (uint32_t)gp + 1u;
@@ -302,10 +306,13 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
         for (int c = 0; c < kUnitPhases; ++c) {
           if (c < k) {
             if (s_px[c]) unit_next_block(s_px[c] - 1u, t, (uint32_t)my_slot, unext, c_sweep, a.k0, a.k1);
-            if (s_item[c] >> 31)
-              dacc += item_unit<kUnitW, P>(s_item[c] & 0xFFFFu, (s_item[c] >> 16) & 0xFu, t, (uint32_t)my_slot,
-                                           my_sp_o, my_sp_o + (uint32_t)n_pos, (uint32_t)L.nbr, ubuf, thr_o,
-                                           c_second, a.k0, a.k1);
+            if (s_item[c] >> 31) {
+              const uint32_t item = s_item[c] & 0x3FFFu;
+              const uint32_t own_o = my_sp_o + 4u * ((s_item[c] >> 18) & 0x1FFFu) + ((item * P) & 3u);
+              dacc += item_unit<kUnitW, P>(item, (s_item[c] >> 14) & 0xFu, t, (uint32_t)my_slot, own_o,
+                                           own_o + (uint32_t)n_pos, (uint32_t)L.nbr, ubuf, thr_o, c_second, a.k0,
+                                           a.k1);
+            }
             __syncthreads();
           }
         }
@@ -391,15 +398,16 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
       __syncthreads();
     }
     if constexpr (kUnit) {
-      // the same copy from the 0/1 bytes (b -> 1 - 2b: 0 -> 0x01, 1 -> 0xFF)
-      const int chunks = n_pos / 16;
-      uint4* dst = reinterpret_cast<uint4*>(a.best_spins + (size_t)s0 * n_pos);
-      for (int i = tid; i < nloc * chunks; i += B) {
-        const int sl = i / chunks;
+      // the same copy from the 0/1 bytes in storage order (b -> 1 - 2b: 0 -> 0x01, 1 -> 0xFF)
+      const uint16_t* place = reinterpret_cast<const uint16_t*>(smem + L.h);
+      const int words = n_pos / 4;
+      uint32_t* dst = reinterpret_cast<uint32_t*>(a.best_spins + (size_t)s0 * n_pos);
+      for (int i = tid; i < nloc * words; i += B) {
+        const int sl = i / words;
         if (imp[sl]) {
-          const uint4 v = *reinterpret_cast<const uint4*>(sp + (size_t)sl * sp_stride + 16 * (i - sl * chunks));
-          dst[i] = make_uint4((v.x * 0xFEu) ^ 0x01010101u, (v.y * 0xFEu) ^ 0x01010101u, (v.z * 0xFEu) ^ 0x01010101u,
-                              (v.w * 0xFEu) ^ 0x01010101u);
+          const uint32_t v =
+              *reinterpret_cast<const uint32_t*>(sp + (size_t)sl * sp_stride + 4 * (size_t)place[i - sl * words]);
+          dst[i] = (v * 0xFEu) ^ 0x01010101u;
         }
       }
     } else {
@@ -523,13 +531,14 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
   if constexpr (kCluster) cl_sync_full();
   __syncthreads();
   if constexpr (kUnit) {
-    const int chunks = n_pos / 16;
-    uint4* dst = reinterpret_cast<uint4*>(a.spins + (size_t)s0 * n_pos);
-    for (int i = tid; i < nloc * chunks; i += B) {
-      const int sl = i / chunks;
-      const uint4 v = *reinterpret_cast<const uint4*>(sp + (size_t)sl * sp_stride + 16 * (i - sl * chunks));
-      dst[i] = make_uint4((v.x * 0xFEu) ^ 0x01010101u, (v.y * 0xFEu) ^ 0x01010101u, (v.z * 0xFEu) ^ 0x01010101u,
-                          (v.w * 0xFEu) ^ 0x01010101u);
+    const uint16_t* place = reinterpret_cast<const uint16_t*>(smem + L.h);
+    const int words = n_pos / 4;
+    uint32_t* dst = reinterpret_cast<uint32_t*>(a.spins + (size_t)s0 * n_pos);
+    for (int i = tid; i < nloc * words; i += B) {
+      const int sl = i / words;
+      const uint32_t v =
+          *reinterpret_cast<const uint32_t*>(sp + (size_t)sl * sp_stride + 4 * (size_t)place[i - sl * words]);
+      dst[i] = (v * 0xFEu) ^ 0x01010101u;
     }
   } else {
     const int4* src = reinterpret_cast<const int4*>(sp);

@@ -15,6 +15,7 @@ struct PtKernelArgs {
   const int* ell_nbr;
   const void* ell_w;
   const void* h_pos;
+  const uint16_t* unit_place;  // unit-regular form: storage word of each 4-position word, or NULL
   // ladder and run
   int R, rpc, spr, n_rounds;
   long long round0;
@@ -94,7 +95,7 @@ __host__ __device__ inline SmemLayout smem_layout(int n_pos, int rpc, int R, int
     // neighbour addresses: (n_pos / P) item rows; Philox blocks: [2][n_pos / 8] x 16 bytes
     L.nbr = o; o = align16(o + (size_t)(n_pos / unit_p) * unit_row_bytes(unit_p, unit_w));
     L.w = o;   o = align16(o + 2 * 16 * (size_t)(n_pos / 8));
-    L.h = o;
+    L.h = o;   o = align16(o + 2 * (size_t)(n_pos / 4));  // storage word of each 4-position word
   } else if (ell_in_smem) {
     L.soff = o; o = align16(o + 4 * (size_t)(n_slices + 1));
     L.nbr = o;  o = align16(o + 4 * (size_t)n_ell);  // integer path: packed neighbour | weight << 24

@@ -192,7 +192,8 @@ __device__ __forceinline__ void sts_u128(uint32_t off, uint4 v) { *reinterpret_c
 
 // One item of the unit-regular form: positions 8g + P j .. 8g + P j + P - 1 (P = 2 or 4) of one
 // replica slot, on a problem whose spins all have W couplings of +-1 and no field.
-//  * The slot's spins are bytes b (0 for +1, 1 for -1) at b_o and their flipped copy b ^ 1 at nb_o.
+//  * The slot's spins are bytes b (0 for +1, 1 for -1) and their flipped copy b ^ 1, at the addresses
+//    the neighbour-address rows and own_o / own_nb_o give.
 //  * The item's row of the neighbour-address table (desc_o, unit_row_bytes(P, W) bytes per item)
 //    holds, for each position i and coupling d, the 16-bit shared address of the byte that neighbour
 //    contributes: its b for a +1 coupling, its b ^ 1 for a -1 coupling. So J s_nb = 1 - 2 byte and
@@ -205,9 +206,11 @@ __device__ __forceinline__ void sts_u128(uint32_t off, uint4 v) { *reinterpret_c
 // runs the same chain bit for bit.
 // The item is given by its index (item = g NI + j, NI = 8 / P items per group) and the mask of its
 // positions that lie in the phase's colour class.
+// own_o / own_nb_o: the shared addresses of the item's P bytes in the b and b ^ 1 arrays (the
+// storage order of words may differ from the position order; a word keeps its 4 positions in order).
 template <int W, int P>
-__device__ __forceinline__ int item_unit(uint32_t item, uint32_t inmask, uint32_t t, uint32_t slot, uint32_t b_o,
-                                         uint32_t nb_o, uint32_t desc_o, uint32_t ubuf_o, uint32_t tab_o,
+__device__ __forceinline__ int item_unit(uint32_t item, uint32_t inmask, uint32_t t, uint32_t slot, uint32_t own_o,
+                                         uint32_t own_nb_o, uint32_t desc_o, uint32_t ubuf_o, uint32_t tab_o,
                                          uint32_t c_second, uint32_t k0, uint32_t k1) {
   static_assert(P == 2 || P == 4, "positions per item");
   constexpr int NI = kGroup / P;
@@ -241,7 +244,6 @@ __device__ __forceinline__ int item_unit(uint32_t item, uint32_t inmask, uint32_
   uint32_t nbv[P * W];
 #pragma unroll
   for (int k = 0; k < P * W; ++k) nbv[k] = lds_u8(a16[k]);
-  const uint32_t own_o = b_o + (uint32_t)p0;
   uint32_t own = P == 2 ? lds_u16(own_o) : lds_u32(own_o);
   uint32_t words[P / 2];
   if constexpr (P == 2) {
@@ -294,10 +296,10 @@ __device__ __forceinline__ int item_unit(uint32_t item, uint32_t inmask, uint32_
     own ^= ((flips * 0x00204081u) & 0x01010101u);
     if constexpr (P == 2) {
       sts_u16(own_o, own);
-      sts_u16(nb_o + (uint32_t)p0, own ^ 0x0101u);
+      sts_u16(own_nb_o, own ^ 0x0101u);
     } else {
       sts_u32(own_o, own);
-      sts_u32(nb_o + (uint32_t)p0, own ^ 0x01010101u);
+      sts_u32(own_nb_o, own ^ 0x01010101u);
     }
   }
   return dacc;

@@ -111,17 +111,25 @@ class DeviceProblem:
         self.max_width = int(np.max(np.diff(slice_off))) if slice_off.size > 1 else 0
         self.min_width = int(np.min(np.diff(slice_off))) if slice_off.size > 1 else 0
         self.unit_regular = int(info.unit_regular) if integer_path else 0
+        # the unit-regular form's bank-aware storage order of the spin bytes (drift_pt_unit_placement)
+        self.unit_place = None
+        if self.unit_regular:
+            place = np.zeros(info.n_pos // 4, np.uint16)
+            _lib.check(L.drift_pt_unit_placement(C.byref(csr), 0, _ptr(place)), "unit_placement")
+            self.unit_place = place
         self.device = torch.device(device)
         t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(self.device)
         self.d_color_ptr, self.d_slice_off, self.d_ell_nbr = t(color_ptr), t(slice_off), t(ell_nbr)
         self.d_ell_w, self.d_h_pos = t(ell_w), t(h_pos)
+        self.d_unit_place = t(self.unit_place.view(np.int16)) if self.unit_place is not None else None
 
     def c_problem(self) -> _lib.DeviceProblem:
         return _lib.DeviceProblem(self.n, self.n_pos, self.n_slices, self.info.n_colors, 1 if self.integer_path else 0,
                                   self.max_field, self.max_width, self.max_class, self.info.has_field,
                                   self.min_width, self.unit_regular, self.n_ell,
                                   self.d_color_ptr.data_ptr(), self.d_slice_off.data_ptr(), self.d_ell_nbr.data_ptr(),
-                                  self.d_ell_w.data_ptr(), self.d_h_pos.data_ptr())
+                                  self.d_ell_w.data_ptr(), self.d_h_pos.data_ptr(),
+                                  self.d_unit_place.data_ptr() if self.d_unit_place is not None else None)
 
     def energy_scale(self) -> float:
         return 1.0 if self.integer_path else 2.0 ** -32

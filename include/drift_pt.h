@@ -114,6 +114,15 @@ typedef struct DriftPtLayout { /* caller-allocated arrays, sized from DriftPtLay
 
 DRIFT_PT_API int drift_pt_layout_fill(const DriftPtCsr* csr, int32_t integer_path, DriftPtLayout* out);
 
+/* Storage order of the unit-regular form's spin bytes in shared memory: word_slot[n_pos / 4]
+ * receives, for the 4-byte word of positions 4u .. 4u+3, the shared-memory word it is stored in
+ * (a permutation of 0 .. n_pos/4 - 1), chosen so that the neighbour gathers of the form's items
+ * (positions_per_item 2 or 4; 0 = the form's own choice) fall on few banks at a time. Pass it as
+ * DriftPtDeviceProblem.unit_place; any permutation gives the same chain bit for bit, only the
+ * shared-memory conflicts differ. Host function; DRIFT_PT_EUNSUPPORTED if the problem is not
+ * unit-regular. No counterpart in the reference. */
+DRIFT_PT_API int drift_pt_unit_placement(const DriftPtCsr* csr, int32_t positions_per_item, uint16_t* word_slot);
+
 /* Metropolis thresholds of the integer path, thr[r*F + x-1] = floor(exp(-2 x beta_r) 2^32)
  * (saturated at 2^32-1) for x = 1..F. Host function. Replaces the per-attempt expf of
  * cuda/ising_pt.cu:118. */
@@ -138,6 +147,8 @@ typedef struct DriftPtDeviceProblem {
   const int32_t* ell_nbr;
   const void* ell_w;
   const void* h_pos;
+  const uint16_t* unit_place;  /* [n_pos/4] from drift_pt_unit_placement, or NULL (positions in order);
+                                  used by the unit-regular form only                            */
 } DriftPtDeviceProblem;
 
 /* Replica state, indexed by replica *slot*. Slots keep their configuration; replica exchange

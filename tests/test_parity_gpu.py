@@ -235,6 +235,28 @@ def test_unit_regular_form_matches_oracle_bit_exact(name):
     assert_bit_exact(st, ost, hist, rounds)
 
 
+def test_unit_regular_form_with_and_without_the_bank_placement():
+    """The storage order of the spin words (drift_pt_unit_placement, on by default) changes no bit."""
+    import torch
+
+    model = maxcut_3regular(4096, 6)
+    betas = geometric_betas(16, 0.25, 5.0)
+    hp = HostProblem.from_model(model)
+    ost = oracle.pt_run(oracle_problem(hp, True), betas, n_rounds=12, sweeps_per_round=2, seed=21,
+                        thr=oracle.thresholds(betas, 3))
+    for placed in (True, False):
+        prob = DeviceProblem(hp)
+        assert prob.d_unit_place is not None
+        if not placed:
+            prob.d_unit_place = None
+        eng = PtEngine(prob, betas, seed=21, sweeps_per_round=2, item_form=2, round_sync=1)
+        eng.init()
+        hist = torch.zeros(12, dtype=torch.float64, device="cuda")
+        eng.run(12, history=hist)
+        eng.check()
+        assert_bit_exact(eng.fetch(), ost, hist.cpu().numpy(), 12)
+
+
 def test_unit_regular_form_resumes_and_checks_its_energy():
     model = maxcut_3regular(1024, 8)
     betas = geometric_betas(32, 0.25, 5.0)
