@@ -73,6 +73,14 @@ WORKLOADS = {
     # dense SK: J_ij ~ N(0, 1)/sqrt(N) (fp32 values) on the upper triangle, mirrored, h = 0, seed 4;
     # 64 replicas, beta 0.3-3.0, rounds of 10 sweeps; 1e4 sweeps per step. Tensor-core field
     # updates: the algorithmic work of an attempt is the 2N flops of J_i . s (drift/ising.py:68)
+    # training of the proposal network of the dense workload: MADE 512-1024-1024-512 (bf16 weights,
+    # fp32 accumulation), Adam on batches of 512 configurations; one step = 50 Adam steps. Algorithmic
+    # work per Adam step: forward 2B(n h1 + h1 h2 + h2 n), the weight gradients the same again, the
+    # activation gradients 2B(h2 n + h1 h2)
+    "made_train": dict(desc="MADE 512-1024-1024-512 training (bf16 x bf16 -> fp32 tensor-core GEMMs), batch 512, "
+                            "50 Adam steps per step", n=512, h=1024, batch=512, adam_steps=50,
+                       flops_per_adam_step=2 * 512 * (2 * (512 * 1024 + 1024 * 1024 + 1024 * 512)
+                                                       + (1024 * 512 + 1024 * 1024))),
     "sk512": dict(desc="SK N=512, J~N(0,1/N) fp32, 64 replicas, beta 0.3-3.0, 1e4 sweeps in rounds of 10",
                   n=512, seed=4, R=64, beta=(0.3, 3.0), sweeps=10000, spr=10, flops_per_attempt=2 * 512),
 }
@@ -1307,7 +1315,71 @@ def main():
         run_workload(args)
 
 
+def bench_made_train(args):
+    """Adam steps of the proposal network at the dense workload's shape (tensor-core GEMMs plus the
+    element-wise training kernels), CUDA events around each step of 50 Adam steps."""
+    import torch
+
+    from drift_b200.made import Made
+
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    w = WORKLOADS[args.workload]
+    n, h, B, K = w["n"], w["h"], w["batch"], w["adam_steps"]
+    made = Made(n, (h, h), seed=1, device=dev)
+    g = torch.Generator(device=dev).manual_seed(5)
+    data = (torch.randint(0, 2, (8 * B, n), device=dev, generator=g) * 2 - 1).to(torch.int8)
+    ev = []
+
+    def step(s_):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        made.train_async(data, steps=K, batch=B, lr=1e-4, seed=s_)
+        e1.record()
+        ev.append((e0, e1))
+
+    for s_ in range(args.warmup):
+        step(s_)
+    made.check()
+    ev.clear()
+    sampler = ClockSampler(local)
+    sampler.start()
+    torch.cuda.synchronize()
+    for s_ in range(args.steps):
+        step(100 + s_)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    made.check()
+    t = sum(a.elapsed_time(b) for a, b in ev) * 1e-3
+    t_max = reduce_max(t, world, dev)
+    flops = float(w["flops_per_adam_step"]) * K * args.steps * world
+    if rank == 0:
+        peak, peak_kind = load_tensor_peak()
+        achieved = flops / t_max / 1e12
+        emit(args, {
+            "metric": "MADE training TFLOP/s", "value": achieved, "unit": "TFLOP/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16 x bf16 -> fp32",
+            "data": "synthetic (random +-1 configurations)",
+            "config": {"workload": w["desc"], "adam_steps_per_step": K, "flops_per_adam_step": w["flops_per_adam_step"]},
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "the whole Adam step (gemm_bf16_kernel and the element-wise training kernels)"},
+            # per Adam step: spins to bf16, 3 forward and 5 backward GEMMs, the loss, 6 transposes, 3 bias
+            # sums, 6 Adam updates
+            "gpu_launches": 25 * K * args.steps, "clocks": clocks,
+        })
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
 def run_workload(args):
+    if args.workload == "made_train":
+        bench_made_train(args)
+        return
     if args.workload == "batched_er":
         bench_batched(args)
     elif args.workload == "sk512":
