@@ -517,6 +517,7 @@ SECONDARIES = [
     ("ea3d64_C5", "ea3d64", {}),
     ("ea2d_batch256_C5b", "ea2d_batch256", {}),
     ("maxcut3reg_r2048", "maxcut3reg_r2048", {}),
+    ("made_train_C4_network", "made_train", {}),
 ]
 # the reference's own GPU engine (cuda/ising_pt.cu built unchanged into oracle/_ref) on shortened jobs
 REFERENCE_GPU = [("maxcut3reg_C2", "maxcut3reg", 2500), ("ea2d_C1", "ea2d", 20000)]

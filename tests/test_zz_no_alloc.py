@@ -119,16 +119,24 @@ def test_noalloc_entry_at_its_replica_limit():
 
 
 def test_noalloc_check_reports_a_wait_that_ran_out():
-    """A wait limit of 1 ns runs out at the first grid-wide wait; the kernel gives up (it sets the
-    error flag, every CTA leaves its round loop) and the check reports it. The next call with the
-    default limit starts from a cleared scratch and is clean."""
+    """A wait limit of 1 ns runs out at the first grid-wide wait that is not satisfied at once; the
+    kernel gives up (it sets the error flag, every CTA leaves its round loop) and the check reports it.
+    A run only waits when some CTA reaches a round end noticeably before another (about a microsecond
+    of skew), which happened in every one of 30 fresh-process trials of this shape on B200 but is not
+    certain, so up to five runs are made; each that does not time out must report success. The next
+    call with the default limit starts from a cleared scratch and is clean."""
     model = maxcut_3regular(1024, 4)
     prob = DeviceProblem(HostProblem.from_model(model))
     betas = geometric_betas(32, 0.25, 5.0)
     eng = PtEngine(prob, betas, seed=9, sweeps_per_round=1, replicas_per_cta=1, round_sync=1)
-    eng.init()
-    _run_noalloc(eng, 200, timeout_s=1e-9)
-    rc = _noalloc_check(eng)
+    rc = _lib.OK
+    for _ in range(5):
+        eng.init()
+        _run_noalloc(eng, 2000, timeout_s=1e-9)
+        rc = _noalloc_check(eng)
+        if rc == _lib.ETIMEOUT:
+            break
+        assert rc == _lib.OK, rc
     assert rc == _lib.ETIMEOUT, rc
     assert "timed out" in _lib.load().drift_pt_last_error().decode()
     eng.init()
