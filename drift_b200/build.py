@@ -60,14 +60,20 @@ def build_cli(force: bool = False, verbose: bool = False) -> str:
     return CLI_PATH
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
+# A profiling build of the same sources with the dense kernel's hand-off stamps compiled in
+# (drift_b200/sk_stamps.py reads them); the product library never has them.
+SK_STAMP_LIB_PATH = os.path.join(HERE, "libdrift_pt_skstamp.so")
+
+
+def build(force: bool = False, verbose: bool = False, sk_stamps: bool = False) -> str:
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
     deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
     deps.append(os.path.join(os.path.dirname(HERE), "include", "drift_pt.h"))
-    if not force and not _stale(LIB_PATH, deps):
-        return LIB_PATH
-    tmp = LIB_PATH + ".tmp"
-    cmd = [nvcc(), "-O3", "-std=c++17", *ARCH_FLAGS, "-lineinfo", "-shared",
+    out = SK_STAMP_LIB_PATH if sk_stamps else LIB_PATH
+    if not force and not _stale(out, deps):
+        return out
+    tmp = out + ".tmp"
+    cmd = [nvcc(), "-O3", "-std=c++17", *ARCH_FLAGS, "-lineinfo", "-shared", *(["-DDPT_SK_STAMPS"] if sk_stamps else []),
            "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-Xcompiler", "-fvisibility=hidden",
            "--expt-relaxed-constexpr", "-o", tmp, *srcs]
     if verbose:
@@ -75,10 +81,13 @@ def build(force: bool = False, verbose: bool = False) -> str:
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed ({r.returncode}):\n{r.stdout}\n{r.stderr}")
-    os.replace(tmp, LIB_PATH)
-    return LIB_PATH
+    os.replace(tmp, out)
+    return out
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose=True))
-    print(build_cli(force="--force" in sys.argv, verbose=True))
+    if "--sk-stamps" in sys.argv:
+        print(build(force="--force" in sys.argv, verbose=True, sk_stamps=True))
+    else:
+        print(build(force="--force" in sys.argv, verbose=True))
+        print(build_cli(force="--force" in sys.argv, verbose=True))

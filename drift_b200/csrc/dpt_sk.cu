@@ -29,6 +29,28 @@
 #include "dpt_internal.h"
 #include "dpt_sk.h"
 
+// Profiling build only (-DDPT_SK_STAMPS, `python -m drift_b200.build --sk-stamps`): clock64 stamps of
+// CTA 0 at each hand-off of a block (resolver 0 picks up block j, resolver 0 publishes its delta,
+// the producer sees all deltas, the loaders' reads of the set are done, the MMAs are committed, a
+// loader sees block j-2's MMAs, a loader releases block j's stage), read back by drift_pt_sk_stamps
+// (drift_b200/sk_stamps.py). The product build compiles the stamps to nothing.
+#ifdef DPT_SK_STAMPS
+namespace dpt {
+__device__ unsigned long long g_sk_stamp[8][4096];
+}
+#define SK_STAMP(e, j)                                                        \
+  do {                                                                        \
+    if (blockIdx.x == 0 && (j) < 4096) ::dpt::g_sk_stamp[e][j] = clock64(); \
+  } while (0)
+extern "C" DRIFT_PT_API int drift_pt_sk_stamps(unsigned long long* out) {
+  return cudaMemcpyFromSymbol(out, dpt::g_sk_stamp, sizeof(dpt::g_sk_stamp)) == cudaSuccess ? 0 : DRIFT_PT_ECUDA;
+}
+#else
+#define SK_STAMP(e, j) \
+  do {                 \
+  } while (0)
+#endif
+
 namespace dpt {
 namespace {
 
@@ -410,6 +432,7 @@ __global__ void __launch_bounds__(kSkThreads, 1) sk_run_kernel(const SkArgs a) {
       for (int j = 0; j < a.n_steps; ++j) {
         // block j staged: fields complete up to block j-2, thresholds, coupling entry in the ring
         if (!wait_stage(stage + (j & 3), j + 1, ctl)) break;
+        if (r == 0 && lane == 0) SK_STAMP(0, j);
         int32_t F = fields[((j & 3) * G + r) * kBlock + lane];
         const int32_t D = thr[((j & 3) * G + r) * kBlock + lane];
         const int32_t* dg = reinterpret_cast<const int32_t*>(ring + (size_t)(j % kRing) * EB +
@@ -472,6 +495,7 @@ __global__ void __launch_bounds__(kSkThreads, 1) sk_run_kernel(const SkArgs a) {
         fence_async_smem();
         __syncwarp();
         if (lane == 0) mbar_arrive(bar(kBarDelta + (j & 3)));
+        if (r == 0 && lane == 0) SK_STAMP(1, j);
         pmask = fl;
         psign = sb;
         // ---- round end: best, then publish the energy for the exchange ----
@@ -620,6 +644,7 @@ __global__ void __launch_bounds__(kSkThreads, 1) sk_run_kernel(const SkArgs a) {
       uint32_t* fb = reinterpret_cast<uint32_t*>(fields) + (size_t)(j & 3) * G * kBlock + lane;
       // first read: the set of block j-1's parity, complete up to block j-3
       if (j >= 3 && !wait_warp(bar(kBarMma + ((j - 3) & 3)), (uint32_t)((j - 3) >> 2) & 1u, ctl)) break;
+      if (lane == 0) SK_STAMP(7, j);
       tc_after();
       {
         const int set = (j - 1) & 1;
@@ -655,6 +680,7 @@ __global__ void __launch_bounds__(kSkThreads, 1) sk_run_kernel(const SkArgs a) {
       }
       // second read: the set of block j's parity, complete up to block j-2
       if (j >= 2 && !wait_warp(bar(kBarMma + ((j - 2) & 3)), (uint32_t)((j - 2) >> 2) & 1u, ctl)) break;
+      if (lane == 0) SK_STAMP(5, j);
       tc_after();
       {
         const int set = j & 1;
@@ -675,6 +701,7 @@ __global__ void __launch_bounds__(kSkThreads, 1) sk_run_kernel(const SkArgs a) {
         if (!wait_warp(bar(kBarSlabFull + b), (uint32_t)(n_init + j / kRing) & 1u, ctl)) break;
       }
       __syncwarp();
+      if (lane == 0) SK_STAMP(6, j);
       if (lane == 0) st_release_cta(stage + (j & 3), j + 1);
     }
     // the exchange that ends the last round
@@ -729,11 +756,14 @@ __global__ void __launch_bounds__(kSkThreads, 1) sk_run_kernel(const SkArgs a) {
           }
           if (i <= n_steps - 3) {  // the last two blocks' products are never read
             if (!wait1(bar(kBarDelta + (i & 3)), (uint32_t)(i >> 2) & 1u, ctl)) break;
+            SK_STAMP(2, i);
             if (!wait1(bar(kBarRead + (i & 3)), (uint32_t)(i >> 2) & 1u, ctl)) break;
+            SK_STAMP(3, i);
             if (!wait_full(i % kRing)) break;
             tc_after();
             issue(i & 1, i % kRing, delta_a + (uint32_t)((i & 3) * kOpBytes), 1u);
             mma_commit(bar(kBarMma + (i & 3)));
+            SK_STAMP(4, i);
           }
         }
       }
