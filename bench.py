@@ -464,8 +464,11 @@ def bench_b200(args):
     e2e_steps = max(1, min(args.steps, 5))
     barrier(world)
     t0 = time.perf_counter()
+    solve_ms = []  # per call: wall time, and the device time of its kernel as the call reports it
     for _ in range(e2e_steps):
+        t1 = time.perf_counter()
         _lib.check(L.drift_pt_solve(C.byref(csr), C.byref(sa), C.byref(sr)), "drift_pt_solve")
+        solve_ms.append([round((time.perf_counter() - t1) * 1e3, 2), round(sr.seconds * 1e3, 2)])
     t_e2e = reduce_max(time.perf_counter() - t0, world, dev)
     e2e = attempts_per_step * e2e_steps * world / t_e2e / 1e9
     info = prob.info
@@ -494,13 +497,14 @@ def bench_b200(args):
                          "kernel": "pt_run_kernel", "bytes_per_attempt": w["bytes_per_attempt"],
                          "kernel_ms": launch_s * 1e3},
             "e2e": {"value": e2e, "unit": "flips/ns", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                    "api": "drift_pt_solve (C ABI, host buffers)"},
+                    "api": "drift_pt_solve (C ABI, host buffers)", "solve_wall_and_kernel_ms": solve_ms},
             "gpu_launches": 4 * args.steps,
             "clocks": clocks,
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_oracle(w, args.workload)
-        if world == 1 and args.workload == "maxcut3reg" and not args.no_secondary and not args.rounds:
+        if (world == 1 and args.workload == "maxcut3reg" and not args.no_secondary and not args.rounds
+                and not getattr(args, "sweeps_per_round", 0)):
             line["secondary"] = secondaries(args)
         emit(args, line)
     if world > 1:
@@ -1307,7 +1311,15 @@ def main():
                     help="override the rounds per step (profiling of a short case; the line then says so)")
     ap.add_argument("--no-secondary", action="store_true",
                     help="default workload: skip the other workloads' lines (the 'secondary' object)")
+    ap.add_argument("--sweeps-per-round", type=int, default=0,
+                    help="sparse workloads: override the sweeps per round (same sweeps per job; the line then says so)")
     args = ap.parse_args()
+    if args.sweeps_per_round:
+        w = WORKLOADS[args.workload]
+        if args.workload not in ("maxcut3reg", "ea2d"):
+            ap.error("--sweeps-per-round applies to the maxcut3reg and ea2d workloads")
+        WORKLOADS[args.workload] = dict(w, spr=args.sweeps_per_round,
+                                        desc=w["desc"] + f" [{args.sweeps_per_round} sweeps per round]")
     if args.impl == "reference":
         bench_reference(args)
     elif args.impl == "reference-gpu":

@@ -262,7 +262,7 @@ int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPl
   lp->cluster = 0;
   lp->unit = 0;
 
-  // ---- the unit-regular form: one replica slot per CTA, 8 positions per item, neighbour addresses
+  // ---- the unit-regular form: one replica slot per CTA, 2 or 4 positions per item, neighbour addresses
   // and the decision table staged in shared memory (problems whose spins all have W couplings of
   // +-1 and no field) ----
   const int form = r->item_form;
@@ -271,16 +271,15 @@ int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPl
                        p->max_field == p->max_width && unit_width_supported(p->max_width) &&
                        r->replicas_per_cta <= 1 && (P_user == 0 || P_user == 2 || P_user == 4) &&
                        p->n_colors <= kUnitPhases && 2 * (long long)p->n_pos + 16 <= 65536 &&
+                       r->sweeps_per_round <= (1 << 23) &&
                        (p->max_class + 14) / kGroup * 2 <= kMaxUnitThreads;
   if (form == 2 && !unit_ok)
     return set_error(DRIFT_PT_EUNSUPPORTED,
                      "item_form 2 needs a unit-regular problem (every spin with the same number, 2, 3, 4 or 6, of "
                      "+-1 couplings, no field, at most 32760 positions, at most 4 colour classes of at most 4080 "
-                     "spins), one replica per CTA and 2 or 4 positions per item");
+                     "spins), at most 2^23 sweeps per round, one replica per CTA and 2 or 4 positions per item");
   if (P_user == 2 && (!unit_ok || form == 1))
     return set_error(DRIFT_PT_EINVAL, "positions_per_item 2 exists in the unit-regular form only");
-  LaunchPlan unit_grid{};
-  bool have_unit_grid = false;
   if (unit_ok && form != 1) {
     const int W = p->max_width;
     // items of the largest colour class: a class of m positions touches at most (m + 14) / 8 groups
@@ -315,14 +314,10 @@ int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPl
         rc = prepare_kernel(fn, threads, smem, &per_sm);
         if (rc) return rc;
         if ((long long)per_sm * di.sm_count >= R) {
-          unit_grid = LaunchPlan{1, threads, 1, R, PU, 0, 1, smem};
-          have_unit_grid = true;
-          // chosen here unless the automatic shape may still pick a cluster form below (small
-          // ladders, where the cluster form's shorter round end is worth more than the item form)
-          if (form == 2 || mode == 1 || R > 2 * kMaxCluster) {
-            *lp = unit_grid;
-            return DRIFT_PT_OK;
-          }
+          // Chosen over every form of the gather: on B200 it ran 2-D EA L = 16 with 24 replicas and a
+          // swap after every sweep at 3.4 attempts/ns against 2.6 for the gather's cluster form.
+          *lp = LaunchPlan{1, threads, 1, R, PU, 0, 1, smem};
+          return DRIFT_PT_OK;
         }
       }
     }
@@ -330,15 +325,6 @@ int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPl
       return set_error(DRIFT_PT_EUNSUPPORTED, "item_form 2: no launch shape with one replica per CTA fits (%d replicas, "
                        "%d positions, round_sync %d)", R, p->n_pos, mode);
   }
-  // the unit-regular grid form when no cluster form of the gather is taken (automatic shape only)
-  auto unit_or = [&](auto&& other) -> int {
-    if (have_unit_grid) {
-      *lp = unit_grid;
-      return DRIFT_PT_OK;
-    }
-    return other();
-  };
-
   // ---- the cluster form: the ladder in one cluster of at most 16 CTAs, coupling table in shared
   // memory; a round's energies cross through distributed shared memory behind one barrier ----
   auto try_cluster = [&](int P_, bool require_one_pass, bool* done) -> int {
@@ -454,10 +440,10 @@ int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPl
     rc = try_cluster(1, true, &done);
     if (rc || done) return rc;
   }
-  if (p1_alone && R <= di.sm_count && phases >= 4) return unit_or([&] { return plan_grid(1); });
+  if (p1_alone && R <= di.sm_count && phases >= 4) return plan_grid(1);
   rc = try_cluster(4, true, &done);
   if (rc || done) return rc;
-  return unit_or([&] { return plan_grid(p1_alone && R <= di.sm_count ? 1 : 4); });
+  return plan_grid(p1_alone && R <= di.sm_count ? 1 : 4);
 }
 
 }  // namespace

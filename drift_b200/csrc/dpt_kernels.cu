@@ -75,6 +75,26 @@ __device__ __forceinline__ long long cl_ld_s64(uint32_t caddr) {
   return v;
 }
 
+// The swap test u < exp_neg_d(delta) for delta < 0, u in [0, 1). A single-precision estimate
+// decides it when u lies clearly above or below: __expf's documented error is at most
+// 2 + floor(1.173 |x|) ulp, with the rounding of delta to float below 2^-15.9 relative for
+// |delta| <= 80, and the margin is 2^-12. Otherwise, and for u = 0, exp_neg_d decides, so the
+// outcome is always that of u < exp_neg_d(delta). Below delta = -80, exp_neg_d(delta) < 2^-53, the
+// smallest positive u.
+__device__ __forceinline__ bool swap_accept(double u, double delta) {
+  if (delta >= -80.0) {
+    const double ef = (double)__expf((float)delta);
+    if (u >= ef * (1.0 + 0x1p-12)) return false;
+    if (u < ef * (1.0 - 0x1p-12)) return true;
+  } else if (u > 0.0) {
+    return false;
+  }
+  return u < exp_neg_d(delta);
+}
+
+// polls of a publication word between two reads of the error flag and the clock
+constexpr int kPollCheck = 8;
+
 __device__ __forceinline__ int ld_relaxed_i32(const int* p) {
   int v;
   asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -240,6 +260,20 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
       for (int i = tid; i < n_pos / 4; i += B) d4[i] = s4[i];
     }
   }
+  // Swap uniform of an exchange lane's first pair (parity + 2 lane, lanes 0..31) in round `rnd`: it
+  // depends only on the pair and the round.
+  auto swap_uniform = [&](long long rnd, int lane) -> double {
+    const int pr = (int)(rnd & 1);
+    if (pr + 2 * lane + 1 >= R) return 0.0;
+    const U4 u = philox(U4{(uint32_t)(pr + 2 * lane), (uint32_t)rnd, (uint32_t)((unsigned long long)rnd >> 32),
+                           ctr3(kTagSwap, a.inst)}, a.k0, a.k1);
+    return uniform53(u.x, u.y);
+  };
+  // Unit-regular form with 3 or more warps: warp 2 draws the next round's swap uniforms while warp 0
+  // runs this round's exchange, so they are ready in shared memory (by round parity) when needed.
+  double* usw = reinterpret_cast<double*>(smem + L.usw);
+  const bool unit_helper = kUnit && B >= 96;
+  if (unit_helper && (tid >> 5) == 2) usw[tid & 31] = swap_uniform(a.round0, tid & 31);
   if (tid == 0) {
     ctl[0] = 0;  // abort flag
     long long b = a.best_energy[0];
@@ -250,6 +284,12 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
   if constexpr (!kInt)
     for (int i = tid; i < nloc; i += B) nb_sm[i] = -2.0f * (float)beta_sm[rung_sm[s0 + i]];
   __syncthreads();
+  // unit-regular form (one slot per CTA): every thread keeps the slot's energy and best energy
+  long long e_u = 0, eb_u = 0;
+  if constexpr (kUnit) {
+    e_u = ecur[0];
+    eb_u = ebest[0];
+  }
 
   // Thread -> slot binding: `tps` consecutive threads serve one slot for the whole launch, so each
   // thread keeps its slot's energy change in a register (no atomics in the sweep loop).
@@ -287,9 +327,143 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
       if (gp < (hi + 7) / kGroup) s_px[c] = (uint32_t)gp + 1u;
     }
   }
+  // Grid form: publish slot s's energy of round `round` (tag round + 1) for every CTA.
+  auto publish_energy = [&](long long round, int s, long long e) {
+    const size_t at = (size_t)(round & 1) * R + s;
+    if (a.packed) {
+      // energy and round tag in one single-copy-atomic word: no ordering between two words needed
+      st_relaxed_u64(reinterpret_cast<unsigned long long*>(a.pub) + at,
+                     ((unsigned long long)(uint32_t)(round + 1) << 32) | (uint32_t)(int32_t)e);
+    } else {
+      // the energy, then (release-ordered after it) the round tag that readers poll
+      __stcg(a.pub + at, e);
+      st_release_u64(a.tags + at, (unsigned long long)round + 1ull);
+    }
+  };
+  // Grid form: slot s's energy of round `round`, polled until its tag shows. Every wait is bounded
+  // by the timeout; on expiry, or when another CTA has set the error flag, abort_now is set and
+  // the value is not used. The clock and the error flag are read after the first unsuccessful poll
+  // and then after every kPollCheck-th only: read after every poll they slowed the exchange
+  // measurably (2-D EA L = 16 with 24 replicas: 3.3 against 3.65 attempts/ns).
+  auto poll_energy = [&](long long round, int s, int& abort_now) -> long long {
+    const size_t at = (size_t)(round & 1) * R + s;
+    const unsigned long long want = (unsigned long long)round + 1ull;
+    if (a.packed) {
+      const unsigned long long* pw = reinterpret_cast<const unsigned long long*>(a.pub) + at;
+      const uint32_t tag = (uint32_t)want;
+      unsigned long long v = ld_relaxed_u64(pw);
+      if ((uint32_t)(v >> 32) != tag) {
+        const unsigned long long t0 = global_timer_ns();
+        for (int it = 1; (uint32_t)((v = ld_relaxed_u64(pw)) >> 32) != tag; ++it) {
+          if (it != 1 && it % kPollCheck != 0) continue;
+          if (ld_relaxed_i32(a.err) != 0) { abort_now = 1; break; }
+          if (global_timer_ns() - t0 > (unsigned long long)a.timeout_ns) {
+            atomicExch(a.err, DRIFT_PT_ETIMEOUT);
+            abort_now = 1;
+            break;
+          }
+        }
+      }
+      return (long long)(int32_t)(uint32_t)v;
+    }
+    if (ld_acquire_u64(a.tags + at) < want) {
+      const unsigned long long t0 = global_timer_ns();
+      for (int it = 1; ld_acquire_u64(a.tags + at) < want; ++it) {
+        if (it != 1 && it % kPollCheck != 0) continue;
+        if (ld_relaxed_i32(a.err) != 0) { abort_now = 1; break; }
+        if (global_timer_ns() - t0 > (unsigned long long)a.timeout_ns) {
+          atomicExch(a.err, DRIFT_PT_ETIMEOUT);
+          abort_now = 1;
+          break;
+        }
+      }
+    }
+    return abort_now ? 0ll : __ldcg(a.pub + at);
+  };
+  // The decision of pair (r, r + 1) of round `round` between slots sa (rung r) and sb (rung r + 1)
+  // with energy difference de = E(sa) - E(sb); u_first is the uniform of the lane's first pair.
+  auto decide_pair = [&](long long round, int r, int sa, int sb, long long de, double u_first) {
+    const double ded = kInt ? (double)de : d_mul((double)de, kFloatEnergyScale);
+    const double delta = d_mul(d_sub(beta_sm[r], beta_sm[r + 1]), ded);
+    bool acc = delta >= 0.0;
+    if (!acc) {
+      double u = u_first;  // the first pair of the lane (r < 64)
+      if (r >= 64) {
+        const U4 w = philox(U4{(uint32_t)r, (uint32_t)round, (uint32_t)((unsigned long long)round >> 32),
+                               ctr3(kTagSwap, a.inst)}, a.k0, a.k1);
+        u = uniform53(w.x, w.y);
+      }
+      acc = swap_accept(u, delta);
+    }
+    if (blockIdx.x == 0) {
+      stats[2 * r] += 1;
+      stats[2 * r + 1] += acc ? 1 : 0;
+    }
+    if (acc) {
+      slot_sm[r] = sb;
+      slot_sm[r + 1] = sa;
+      rung_sm[sa] = r + 1;
+      rung_sm[sb] = r;
+    }
+  };
+  // The exchange lane `tid` (< 32) of round `round`: its pairs parity + 2 tid, + 64, ...
+  // `energy(slot)` reads a slot's energy of this round.
+  auto exchange_lane = [&](long long round, double u_first, auto&& energy) {
+    for (int r = (int)(round & 1) + 2 * tid; r + 1 < R; r += 64) {
+      const int sa = slot_sm[r], sb = slot_sm[r + 1];
+      decide_pair(round, r, sa, sb, energy(sa) - energy(sb), u_first);
+    }
+  };
+  // Grid form: the energies of slots sa and sb (none when sb < 0) of round `round`, both polled at
+  // once (bounded as poll_energy).
+  auto poll_pair = [&](long long round, int sa, int sb, long long& ea, long long& eb, int& abort_now) {
+    if (!a.packed) {
+      ea = poll_energy(round, sa, abort_now);
+      eb = (abort_now || sb < 0) ? 0ll : poll_energy(round, sb, abort_now);
+      return;
+    }
+    const unsigned long long* base = reinterpret_cast<const unsigned long long*>(a.pub) + (size_t)(round & 1) * R;
+    const uint32_t tag = (uint32_t)(round + 1);
+    unsigned long long va = ld_relaxed_u64(base + sa);
+    unsigned long long vb = sb >= 0 ? ld_relaxed_u64(base + sb) : (unsigned long long)tag << 32;
+    if ((uint32_t)(va >> 32) != tag || (uint32_t)(vb >> 32) != tag) {
+      const unsigned long long t0 = global_timer_ns();
+      for (int it = 1;; ++it) {
+        const bool need_a = (uint32_t)(va >> 32) != tag, need_b = (uint32_t)(vb >> 32) != tag;
+        if (!need_a && !need_b) break;
+        if (need_a) va = ld_relaxed_u64(base + sa);
+        if (need_b) vb = ld_relaxed_u64(base + sb);  // sb >= 0 here
+        if (it != 1 && it % kPollCheck != 0) continue;
+        if (ld_relaxed_i32(a.err) != 0) { abort_now = 1; break; }
+        if (global_timer_ns() - t0 > (unsigned long long)a.timeout_ns) {
+          atomicExch(a.err, DRIFT_PT_ETIMEOUT);
+          abort_now = 1;
+          break;
+        }
+      }
+    }
+    ea = (long long)(int32_t)(uint32_t)va;
+    eb = (long long)(int32_t)(uint32_t)vb;
+  };
+  // the running best energy after round j (CTA 0, one whole warp)
+  // (history_from takes each lane's minimum over the energies it read)
+  auto history_from = [&](int j, long long m) {
+    for (int off = 16; off > 0; off >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, off));
+    if ((tid & 31) == 0) {
+      long long* rb = reinterpret_cast<long long*>(ctl + 2);
+      rb[0] = min(rb[0], m);
+      a.best_hist[j] = kInt ? (double)rb[0] : d_mul((double)rb[0], kFloatEnergyScale);
+    }
+  };
+  auto best_history = [&](int j, auto&& energy) {
+    long long m = LLONG_MAX;
+    for (int i = tid & 31; i < R; i += 32) m = min(m, (long long)energy(i));
+    history_from(j, m);
+  };
   for (int j = 0; j < a.n_rounds; ++j) {
     const long long round = a.round0 + j;
     long long dacc = 0;
+    int dacc_u = 0;  // unit-regular form: |change| <= 2 W P per phase, spr <= 2^23 keeps it in 32 bits
     const uint32_t thr_o = kUnit ? (uint32_t)L.thr + 16u * (uint32_t)(rung_sm[my_slot] * (kUnitW + 1))
                            : kInt ? (uint32_t)L.thr + 4u * (uint32_t)(rung_sm[my_slot] * (2 * a.F + 1) + a.F) : 0u;
     const float neg2beta = kInt ? 0.0f : nb_sm[active ? my_sl : 0];
@@ -309,220 +483,220 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
             if (s_item[c] >> 31) {
               const uint32_t item = s_item[c] & 0x3FFFu;
               const uint32_t own_o = my_sp_o + 4u * ((s_item[c] >> 18) & 0x1FFFu) + ((item * P) & 3u);
-              dacc += item_unit<kUnitW, P>(item, (s_item[c] >> 14) & 0xFu, t, (uint32_t)my_slot, own_o,
+              dacc_u += item_unit<kUnitW, P>(item, (s_item[c] >> 14) & 0xFu, t, (uint32_t)my_slot, own_o,
                                            own_o + (uint32_t)n_pos, (uint32_t)L.nbr, ubuf, thr_o, c_second, a.k0,
                                            a.k1);
             }
             __syncthreads();
           }
         }
-        continue;
-      }
-      for (int c = 0; c < k; ++c) {
-        const int lo = lo_n, hi = hi_n;
-        {
-          const int cn = c + 1 < k ? c + 1 : 0;
-          lo_n = cptr[cn];
-          hi_n = cptr[cn + 1];
-        }
-        const int glo = lo >> 3, ghi = (hi + 7) >> 3;
-        if constexpr (!kUnit) {
-          // item v -> (group, sub-block): 32 consecutive items are 32 consecutive groups (coalesced
-          // coupling reads), the NB sub-blocks of those groups follow as the next 32-item runs
-          const int span = ((ghi - glo + 31) >> 5) * 32 * NB;
-          if (active) {
-            for (int v = lt; v < span; v += tps) {
-              const int b = (v >> 5) & (NB - 1);
-              const int g = glo + (v / (32 * NB)) * 32 + (v & 31);
-              if (g >= ghi) continue;
-              if constexpr (kInt)
-                dacc += group_int<W, kExactW, kInSmem, kField, P>(g, b, lo, hi, t, (uint32_t)my_slot, my_sp_o, T,
-                                                                  thr_o, c_sweep, c_second, a.k0, a.k1);
-              else
-                dacc += group_f32<W, kExactW, kInSmem, kField>(g, lo, hi, t, (uint32_t)my_slot, my_sp_o, T,
-                                                               neg2beta, c_sweep, c_second, a.k0, a.k1);
-            }
+      } else {
+        for (int c = 0; c < k; ++c) {
+          const int lo = lo_n, hi = hi_n;
+          {
+            const int cn = c + 1 < k ? c + 1 : 0;
+            lo_n = cptr[cn];
+            hi_n = cptr[cn + 1];
           }
-        }
-        __syncthreads();
-      }
-    }
-    // ---- round end ----
-    // The exchange lanes draw the swap uniform of their first pair now: it depends only on the pair
-    // and the round, so its latency hides behind the energy reduction.
-    const int parity = (int)(round & 1);
-    double u_first = 0.0;
-    if (tid < 32 && parity + 2 * tid + 1 < R) {
-      const U4 u = philox(U4{(uint32_t)(parity + 2 * tid), (uint32_t)round, (uint32_t)((unsigned long long)round >> 32),
-                             ctr3(kTagSwap, a.inst)}, a.k0, a.k1);
-      u_first = uniform53(u.x, u.y);
-    }
-    // reduce the energy change of each slot over its threads
-    for (int off = seg >> 1; off > 0; off >>= 1) dacc += __shfl_xor_sync(0xffffffffu, dacc, off);
-    if (lt % seg == 0) eacc[tid / seg] = dacc;
-    __syncthreads();
-    // a slot's nseg <= 32 partial sums are added by one warp (shuffles, not a serial chain of
-    // shared loads); slots are spread over the warps. Integer sums: any order gives the same bits.
-    const int nseg = tps / seg;
-    for (int i = tid >> 5; i < nloc; i += B >> 5) {
-      const int ln = tid & 31;
-      long long part = ln < nseg ? eacc[i * nseg + ln] : 0ll;
-      for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
-      if (ln == 0) {
-      const long long e = ecur[i] + part;
-      ecur[i] = e;
-      imp[i] = (e < ebest[i]) ? 1 : 0;
-      if (e < ebest[i]) ebest[i] = e;
-      if constexpr (kCluster) {
-        cpub[(round & 1) * a.rpc + i] = e;
-      } else if (gridDim.x > 1) {
-        const size_t at = (size_t)(round & 1) * R + s0 + i;
-        if (a.packed) {
-          // energy and round tag in one single-copy-atomic word: no ordering between two words needed
-          st_relaxed_u64(reinterpret_cast<unsigned long long*>(a.pub) + at,
-                         ((unsigned long long)(uint32_t)(round + 1) << 32) | (uint32_t)(int32_t)e);
-        } else {
-          // publish: the energy, then (release-ordered after it) the round tag that readers poll
-          __stcg(a.pub + at, e);
-          st_release_u64(a.tags + at, (unsigned long long)round + 1ull);
-        }
-      }
-      }
-    }
-    if constexpr (kCluster) {
-      // one cluster barrier publishes this round's energies to the other CTAs and, being a barrier
-      // of every thread of the cluster, orders this CTA's own round-end writes for all its threads
-      cl_arrive_smem();
-      cl_wait();
-    } else {
-      __syncthreads();
-    }
-    if constexpr (kUnit) {
-      // the same copy from the 0/1 bytes in storage order (b -> 1 - 2b: 0 -> 0x01, 1 -> 0xFF)
-      const uint16_t* place = reinterpret_cast<const uint16_t*>(smem + L.h);
-      const int words = n_pos / 4;
-      uint32_t* dst = reinterpret_cast<uint32_t*>(a.best_spins + (size_t)s0 * n_pos);
-      for (int i = tid; i < nloc * words; i += B) {
-        const int sl = i / words;
-        if (imp[sl]) {
-          const uint32_t v =
-              *reinterpret_cast<const uint32_t*>(sp + (size_t)sl * sp_stride + 4 * (size_t)place[i - sl * words]);
-          dst[i] = (v * 0xFEu) ^ 0x01010101u;
-        }
-      }
-    } else {
-      // copy the spins of every slot that reached a new best, all slots in one pass
-      const int chunks = n_pos / 16;
-      const int4* src = reinterpret_cast<const int4*>(sp);
-      int4* dst = reinterpret_cast<int4*>(a.best_spins + (size_t)s0 * n_pos);
-      for (int i = tid; i < nloc * chunks; i += B)
-        if (imp[i / chunks]) dst[i] = src[i];
-    }
-    // cluster form: a slot's energy of this round, read from its owner's shared memory
-    const uint32_t cbase = kCluster ? (uint32_t)__cvta_generic_to_shared(cpub + (round & 1) * a.rpc) : 0u;
-    auto cl_energy = [&](int sl) {
-      const int o = sl / a.rpc;
-      return cl_ld_s64(cl_map(cbase + 8u * (uint32_t)(sl - o * a.rpc), (uint32_t)o));
-    };
-    if constexpr (kCluster) {
-      // nothing to gather: the exchange and history warps read the energies they use directly
-    } else if (gridDim.x > 1) {
-      // gather every slot's energy of this round: poll its tag (acquire), then read the energy;
-      // this is the only grid-wide synchronisation of the round, bounded by the timeout
-      int abort_now = 0;
-      const unsigned long long want = (unsigned long long)round + 1ull;
-      for (int s = tid; s < R && !abort_now; s += B) {
-        const size_t at = (size_t)(round & 1) * R + s;
-        if (a.packed) {
-          const unsigned long long* pw = reinterpret_cast<const unsigned long long*>(a.pub) + at;
-          const uint32_t tag = (uint32_t)want;
-          unsigned long long v = ld_relaxed_u64(pw);
-          if ((uint32_t)(v >> 32) != tag) {
-            const unsigned long long t0 = global_timer_ns();
-            while ((uint32_t)((v = ld_relaxed_u64(pw)) >> 32) != tag) {
-              if (ld_relaxed_i32(a.err) != 0) { abort_now = 1; break; }
-              if (global_timer_ns() - t0 > (unsigned long long)a.timeout_ns) {
-                atomicExch(a.err, DRIFT_PT_ETIMEOUT);
-                abort_now = 1;
-                break;
+          const int glo = lo >> 3, ghi = (hi + 7) >> 3;
+          {
+            // item v -> (group, sub-block): 32 consecutive items are 32 consecutive groups (coalesced
+            // coupling reads), the NB sub-blocks of those groups follow as the next 32-item runs
+            const int span = ((ghi - glo + 31) >> 5) * 32 * NB;
+            if (active) {
+              for (int v = lt; v < span; v += tps) {
+                const int b = (v >> 5) & (NB - 1);
+                const int g = glo + (v / (32 * NB)) * 32 + (v & 31);
+                if (g >= ghi) continue;
+                if constexpr (kInt)
+                  dacc += group_int<W, kExactW, kInSmem, kField, P>(g, b, lo, hi, t, (uint32_t)my_slot, my_sp_o, T,
+                                                                    thr_o, c_sweep, c_second, a.k0, a.k1);
+                else
+                  dacc += group_f32<W, kExactW, kInSmem, kField>(g, lo, hi, t, (uint32_t)my_slot, my_sp_o, T,
+                                                                 neg2beta, c_sweep, c_second, a.k0, a.k1);
               }
             }
           }
-          if (!abort_now) eall[s] = (long long)(int32_t)(uint32_t)v;
-          continue;
+          __syncthreads();
         }
-        if (ld_acquire_u64(a.tags + at) < want) {
-          const unsigned long long t0 = global_timer_ns();
-          while (ld_acquire_u64(a.tags + at) < want) {
-            if (ld_relaxed_i32(a.err) != 0) { abort_now = 1; break; }
-            if (global_timer_ns() - t0 > (unsigned long long)a.timeout_ns) {
-              atomicExch(a.err, DRIFT_PT_ETIMEOUT);
-              abort_now = 1;
-              break;
+      }
+    }
+    // ---- round end ----
+    if constexpr (kUnit) {
+      // One slot per CTA. Each warp adds its threads' energy changes as two 32-bit sums, of the low
+      // 16 bits and of the rest, so no sum can overflow; after one barrier every thread adds the
+      // warps' sums itself and holds the slot's new energy. Integer sums: any order, the same bits.
+      const int lane = tid & 31, wid = tid >> 5;
+      double u_first = 0.0;
+      if (!unit_helper && tid < 32) u_first = swap_uniform(round, tid);
+      {
+        const int lo = __reduce_add_sync(0xffffffffu, dacc_u & 0xFFFF);
+        const int hi = __reduce_add_sync(0xffffffffu, dacc_u >> 16);
+        if (lane == 0) reinterpret_cast<int2*>(eacc)[wid] = make_int2(lo, hi);
+      }
+      __syncthreads();
+      {
+        const int2 pw = lane < (B >> 5) ? reinterpret_cast<const int2*>(eacc)[lane] : make_int2(0, 0);
+        const int lo = __reduce_add_sync(0xffffffffu, pw.x), hi = __reduce_add_sync(0xffffffffu, pw.y);
+        e_u += (long long)hi * 65536 + lo;
+      }
+      const bool improved = e_u < eb_u;
+      if (improved) eb_u = e_u;
+      if (tid == 0) {
+        ecur[0] = e_u;
+        ebest[0] = eb_u;
+        if constexpr (kCluster) cpub[(round & 1) * a.rpc] = e_u;
+        else if (gridDim.x > 1) publish_energy(round, s0, e_u);
+        else eall[0] = e_u;
+      }
+      if (improved) {
+        // the spins of the new best, from the 0/1 bytes in storage order (b -> 1 - 2b: 0 -> 0x01,
+        // 1 -> 0xFF); the spins change again only after the round's last barrier
+        const uint16_t* place = reinterpret_cast<const uint16_t*>(smem + L.h);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(a.best_spins + (size_t)s0 * n_pos);
+        for (int i = tid; i < n_pos / 4; i += B)
+          dst[i] = (*reinterpret_cast<const uint32_t*>(sp + 4 * (size_t)place[i]) * 0xFEu) ^ 0x01010101u;
+      }
+      if (unit_helper && tid < 32) u_first = usw[(j & 1) * 32 + tid];
+      if constexpr (kCluster) {
+        // one cluster barrier publishes this round's energies; the exchange and history warps read
+        // them from their owners' shared memory
+        cl_arrive_smem();
+        cl_wait();
+        const uint32_t cbase = (uint32_t)__cvta_generic_to_shared(cpub + (round & 1) * a.rpc);
+        auto cl_energy = [&](int sl) {
+          const int o = sl / a.rpc;
+          return cl_ld_s64(cl_map(cbase + 8u * (uint32_t)(sl - o * a.rpc), (uint32_t)o));
+        };
+        if (tid < 32) exchange_lane(round, u_first, cl_energy);
+        if (blockIdx.x == 0 && a.best_hist && wid == (B > 32 ? 1 : 0)) best_history(j, cl_energy);
+      } else {
+        // With at most 64 slots and 3 or more warps, warp 0 polls every slot's energy (lane l slots
+        // l and l + 32, coalesced), hands each pair's lane its two energies by shuffles and decides
+        // the pairs: no gather into shared memory and no barrier of the whole CTA. In CTA 0, warp 1
+        // polls them as well for the best-energy history. Other shapes gather through shared memory.
+        const bool direct = gridDim.x > 1 && R <= 64 && unit_helper;
+        if (direct) {
+          if (wid == 0) {
+            const int r = (int)(round & 1) + 2 * lane;
+            const bool has = r + 1 < R;
+            const int sa = has ? slot_sm[r] : 0, sb = has ? slot_sm[r + 1] : 0;
+            int abort_now = 0;
+            long long e0 = 0, e1 = 0;
+            poll_pair(round, lane < R ? lane : 0, lane + 32 < R ? lane + 32 : -1, e0, e1, abort_now);
+            // an abort leaves the permutation of the last whole round
+            if (__any_sync(0xffffffffu, abort_now)) {
+              if (lane == 0) ctl[0] = 1;
+            } else {
+              const long long a0 = __shfl_sync(0xffffffffu, e0, sa & 31), a1 = __shfl_sync(0xffffffffu, e1, sa & 31);
+              const long long b0 = __shfl_sync(0xffffffffu, e0, sb & 31), b1 = __shfl_sync(0xffffffffu, e1, sb & 31);
+              if (has) decide_pair(round, r, sa, sb, (sa < 32 ? a0 : a1) - (sb < 32 ? b0 : b1), u_first);
             }
+          } else if (wid == 1 && blockIdx.x == 0 && a.best_hist) {
+            int abort_now = 0;
+            long long e0 = 0, e1 = 0;
+            poll_pair(round, lane < R ? lane : 0, lane + 32 < R ? lane + 32 : -1, e0, e1, abort_now);
+            if (!__any_sync(0xffffffffu, abort_now))
+              history_from(j, min(lane < R ? e0 : LLONG_MAX, lane + 32 < R ? e1 : LLONG_MAX));
+          }
+        } else {
+          if (gridDim.x > 1) {
+            int abort_now = 0;
+            for (int s = tid; s < R && !abort_now; s += B) {
+              const long long e = poll_energy(round, s, abort_now);
+              if (!abort_now) eall[s] = e;
+            }
+            if (abort_now) ctl[0] = 1;
+          }
+          __syncthreads();
+          if (!ctl[0]) {
+            if (tid < 32) exchange_lane(round, u_first, [&](int s) { return eall[s]; });
+            if (blockIdx.x == 0 && a.best_hist && wid == (B > 32 ? 1 : 0)) best_history(j, [&](int s) { return eall[s]; });
           }
         }
-        if (!abort_now) eall[s] = __ldcg(a.pub + at);
       }
-      if (abort_now) ctl[0] = 1;
+      if (unit_helper && wid == 2) usw[((j + 1) & 1) * 32 + lane] = swap_uniform(round + 1, lane);
       __syncthreads();
       if (ctl[0]) break;
     } else {
-      for (int i = tid; i < R; i += B) eall[i] = ecur[i];
-    }
-    if constexpr (!kCluster) __syncthreads();
-    // ---- exchange step: identical in every CTA (disjoint pairs, one lane per pair) ----
-    if (tid < 32) {
-      for (int r = parity + 2 * tid; r + 1 < R; r += 64) {
-        const int sa = slot_sm[r], sb = slot_sm[r + 1];
-        long long de;
-        if constexpr (kCluster) de = cl_energy(sa) - cl_energy(sb);
-        else de = eall[sa] - eall[sb];
-        const double ded = kInt ? (double)de : d_mul((double)de, kFloatEnergyScale);
-        const double delta = d_mul(d_sub(beta_sm[r], beta_sm[r + 1]), ded);
-        bool acc = delta >= 0.0;
-        if (!acc) {
-          double u = u_first;  // the first pair of the lane (r < 64)
-          if (r >= 64) {
-            const U4 w = philox(U4{(uint32_t)r, (uint32_t)round, (uint32_t)((unsigned long long)round >> 32),
-                                   ctr3(kTagSwap, a.inst)}, a.k0, a.k1);
-            u = uniform53(w.x, w.y);
-          }
-          acc = u < exp_neg_d(delta);
-        }
-        if (blockIdx.x == 0) {
-          stats[2 * r] += 1;
-          stats[2 * r + 1] += acc ? 1 : 0;
-        }
-        if (acc) {
-          slot_sm[r] = sb;
-          slot_sm[r + 1] = sa;
-          rung_sm[sa] = r + 1;
-          rung_sm[sb] = r;
-        }
-      }
-    }
-    // best-energy history (CTA 0): warp 1 while warp 0 runs the exchange, or warp 0 after it
-    if (blockIdx.x == 0 && a.best_hist && (tid >> 5) == (B > 32 ? 1 : 0)) {
-      const int lane = tid & 31;
-      long long m = LLONG_MAX;
-      for (int i = lane; i < R; i += 32) {
-        long long e;
-        if constexpr (kCluster) e = cl_energy(i);
-        else e = eall[i];
-        m = min(m, e);
-      }
-      for (int off = 16; off > 0; off >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, off));
-      if (lane == 0) {
-        long long* rb = reinterpret_cast<long long*>(ctl + 2);
-        rb[0] = min(rb[0], m);
-        a.best_hist[j] = kInt ? (double)rb[0] : d_mul((double)rb[0], kFloatEnergyScale);
-      }
-    }
-    __syncthreads();
-    if constexpr (!kInt) {
-      for (int i = tid; i < nloc; i += B) nb_sm[i] = -2.0f * (float)beta_sm[rung_sm[s0 + i]];
+      // The exchange lanes draw the swap uniform of their first pair now: its latency hides behind
+      // the energy reduction.
+      double u_first = 0.0;
+      if (tid < 32) u_first = swap_uniform(round, tid);
+      // reduce the energy change of each slot over its threads
+      for (int off = seg >> 1; off > 0; off >>= 1) dacc += __shfl_xor_sync(0xffffffffu, dacc, off);
+      if (lt % seg == 0) eacc[tid / seg] = dacc;
       __syncthreads();
+      // a slot's nseg <= 32 partial sums are added by one warp (shuffles, not a serial chain of
+      // shared loads); slots are spread over the warps. Integer sums: any order gives the same bits.
+      const int nseg = tps / seg;
+      for (int i = tid >> 5; i < nloc; i += B >> 5) {
+        const int ln = tid & 31;
+        long long part = ln < nseg ? eacc[i * nseg + ln] : 0ll;
+        for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
+        if (ln == 0) {
+          const long long e = ecur[i] + part;
+          ecur[i] = e;
+          imp[i] = (e < ebest[i]) ? 1 : 0;
+          if (e < ebest[i]) ebest[i] = e;
+          if constexpr (kCluster) cpub[(round & 1) * a.rpc + i] = e;
+          else if (gridDim.x > 1) publish_energy(round, s0 + i, e);
+        }
+      }
+      if constexpr (kCluster) {
+        // one cluster barrier publishes this round's energies to the other CTAs and, being a
+        // barrier of every thread of the cluster, orders this CTA's own round-end writes for all
+        // its threads
+        cl_arrive_smem();
+        cl_wait();
+      } else {
+        __syncthreads();
+      }
+      {
+        // copy the spins of every slot that reached a new best, all slots in one pass
+        const int chunks = n_pos / 16;
+        const int4* src = reinterpret_cast<const int4*>(sp);
+        int4* dst = reinterpret_cast<int4*>(a.best_spins + (size_t)s0 * n_pos);
+        for (int i = tid; i < nloc * chunks; i += B)
+          if (imp[i / chunks]) dst[i] = src[i];
+      }
+      // cluster form: a slot's energy of this round, read from its owner's shared memory
+      const uint32_t cbase = kCluster ? (uint32_t)__cvta_generic_to_shared(cpub + (round & 1) * a.rpc) : 0u;
+      auto cl_energy = [&](int sl) {
+        const int o = sl / a.rpc;
+        return cl_ld_s64(cl_map(cbase + 8u * (uint32_t)(sl - o * a.rpc), (uint32_t)o));
+      };
+      if constexpr (kCluster) {
+        // nothing to gather: the exchange and history warps read the energies they use directly
+      } else if (gridDim.x > 1) {
+        // gather every slot's energy of this round: the only grid-wide synchronisation of the round
+        int abort_now = 0;
+        for (int s = tid; s < R && !abort_now; s += B) {
+          const long long e = poll_energy(round, s, abort_now);
+          if (!abort_now) eall[s] = e;
+        }
+        if (abort_now) ctl[0] = 1;
+        __syncthreads();
+        if (ctl[0]) break;
+      } else {
+        for (int i = tid; i < R; i += B) eall[i] = ecur[i];
+        __syncthreads();
+      }
+      // ---- exchange step: identical in every CTA (disjoint pairs, one lane per pair) ----
+      if (tid < 32) {
+        if constexpr (kCluster) exchange_lane(round, u_first, cl_energy);
+        else exchange_lane(round, u_first, [&](int s) { return eall[s]; });
+      }
+      // best-energy history (CTA 0): warp 1 while warp 0 runs the exchange, or warp 0 after it
+      if (blockIdx.x == 0 && a.best_hist && (tid >> 5) == (B > 32 ? 1 : 0)) {
+        if constexpr (kCluster) best_history(j, cl_energy);
+        else best_history(j, [&](int s) { return eall[s]; });
+      }
+      __syncthreads();
+      if constexpr (!kInt) {
+        for (int i = tid; i < nloc; i += B) nb_sm[i] = -2.0f * (float)beta_sm[rung_sm[s0 + i]];
+        __syncthreads();
+      }
     }
   }
 

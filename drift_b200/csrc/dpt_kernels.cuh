@@ -42,7 +42,7 @@ struct PtKernelArgs {
 
 struct SmemLayout {
   size_t spins, eacc, ecur, ebest, imp, eall, rung, slot, beta, nb, thr, stats, cptr, ctl;
-  size_t soff, nbr, w, h, cpub, total;
+  size_t soff, nbr, w, h, cpub, usw, total;
 };
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
@@ -62,7 +62,8 @@ __host__ __device__ inline int seg_width(int threads, int rpc) {
 // (so every spin byte has a 16-bit address); the coupling table is replaced by one row per item of
 // P * W 16-bit neighbour addresses (unit_row_bytes), the threshold rows by the decision table of
 // 2 (W + 1) 64-bit entries per rung, and the Philox blocks of the current and the next sweep are
-// kept per group (2 x 16 bytes per group).
+// kept per group (2 x 16 bytes per group). `usw` holds the swap uniforms of the exchange lanes' first
+// pairs for two rounds (by round parity), drawn a round ahead.
 __host__ __device__ inline size_t unit_slot_bytes(int n_pos) { return 2 * (size_t)n_pos + 16; }
 __host__ __device__ inline int unit_row_bytes(int P, int W) { return ((2 * P * W + 7) / 8) * 8; }
 
@@ -103,6 +104,7 @@ __host__ __device__ inline SmemLayout smem_layout(int n_pos, int rpc, int R, int
     L.h = o;    o = align16(o + 4 * (size_t)n_pos);
   }
   L.cpub = o;   o = align16(o + (cluster ? 16 * (size_t)rpc : 0));
+  L.usw = o;    o = align16(o + (unit_w ? 2 * 32 * sizeof(double) : 0));
   L.total = o;
   return L;
 }
