@@ -171,6 +171,10 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
         self.thread.join(timeout=2)
+        # On B200 boxes, CUDA calls made shortly after an nvidia-smi process exits were seen to stall
+        # for up to ~1 s on the host (kernel time unchanged): let that teardown pass before the next
+        # timed region (the end-to-end calls follow right after).
+        time.sleep(3.0)
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
