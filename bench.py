@@ -127,6 +127,29 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+def issue_basis(kernel_key, attempts_per_s, sm_mhz):
+    """The issue ceiling of a kernel: warp instructions per attempt from its ncu capture
+    (profiles/issue.json) times the measured attempt rate, against 4 warp instructions per SM cycle
+    over the whole chip and over the SMs the launch occupies."""
+    p = os.path.join(ROOT, "profiles", "issue.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f).get(kernel_key)
+    if not d:
+        return None
+    import torch
+
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    hz = float(sm_mhz or 1965.0) * 1e6
+    achieved = attempts_per_s * d["warp_inst_per_attempt"] / 1e9
+    chip = sms * 4 * hz / 1e9
+    used = min(d["ctas"], sms) * 4 * hz / 1e9
+    return {"unit": "G warp instructions/s", "warp_inst_per_attempt": d["warp_inst_per_attempt"], "achieved": achieved,
+            "peak_chip": chip, "frac_chip": achieved / chip, "peak_used_sms": used, "frac_used_sms": achieved / used,
+            "sms_used": min(d["ctas"], sms), "source": "profiles/issue.json (ncu smsp__inst_executed.sum)"}
+
+
 def load_traffic(kernel_key):
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(p):
@@ -486,6 +509,7 @@ def bench_b200(args):
         alg_bytes = attempts_per_step * w["bytes_per_attempt"]
         achieved = alg_bytes / launch_s / 1e9
         traffic = load_traffic(f"pt_run_kernel/{args.workload}")
+        issue = issue_basis(f"pt_run_kernel/{args.workload}", attempts_per_step / launch_s, clocks.get("sm_mhz"))
         line = {
             "metric": "spin-flips/ns", "value": value, "unit": "flips/ns", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
@@ -499,7 +523,7 @@ def bench_b200(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "pt_run_kernel", "bytes_per_attempt": w["bytes_per_attempt"],
-                         "kernel_ms": launch_s * 1e3},
+                         "kernel_ms": launch_s * 1e3, **({"issue": issue} if issue else {})},
             "e2e": {"value": e2e, "unit": "flips/ns", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "api": "drift_pt_solve (C ABI, host buffers)", "solve_wall_and_kernel_ms": solve_ms},
             "gpu_launches": 4 * args.steps,
