@@ -190,6 +190,12 @@ __device__ __forceinline__ void sts_u16(uint32_t off, uint32_t v) { *reinterpret
 __device__ __forceinline__ void sts_u32(uint32_t off, uint32_t v) { *reinterpret_cast<uint32_t*>(dpt_smem + off) = v; }
 __device__ __forceinline__ void sts_u128(uint32_t off, uint4 v) { *reinterpret_cast<uint4*>(dpt_smem + off) = v; }
 
+// The thresholds of a slot's rung for the positive energy changes x = W - 2j, j < (W + 1) / 2
+// (x <= 0 is always accepted), held in registers for the round.
+struct UnitThr {
+  uint32_t t[3];
+};
+
 // One item of the unit-regular form: positions 8g + P j .. 8g + P j + P - 1 (P = 2 or 4) of one
 // replica slot, on a problem whose spins all have W couplings of +-1 and no field.
 //  * The slot's spins are bytes b (0 for +1, 1 for -1) and their flipped copy b ^ 1, at the addresses
@@ -198,8 +204,8 @@ __device__ __forceinline__ void sts_u128(uint32_t off, uint4 v) { *reinterpret_c
 //    holds, for each position i and coupling d, the 16-bit shared address of the byte that neighbour
 //    contributes: its b for a +1 coupling, its b ^ 1 for a -1 coupling. So J s_nb = 1 - 2 byte and
 //    the position's field is W - 2k, k the sum of its W bytes.
-//  * tab_o is the slot's rung row of the decision table: entry (b, k) holds x = (1 - 2b)(W - 2k)
-//    (= s_i field_i, half the flip's energy change) and the threshold of x.
+//  * The position's x = (1 - 2b)(W - 2k) (= s_i field_i, half the flip's energy change) is computed
+//    from b and k; for x > 0 its threshold comes from thr (registers, no shared-memory lookup).
 //  * The uniforms come from the group's Philox block of this sweep, read from ubuf_o (16 bytes per
 //    group); the caller computes the next sweep's blocks separately (unit_next_block).
 // The Metropolis test, the uniforms and the energy change are those of group_int, so every form
@@ -210,7 +216,7 @@ __device__ __forceinline__ void sts_u128(uint32_t off, uint4 v) { *reinterpret_c
 // storage order of words may differ from the position order; a word keeps its 4 positions in order).
 template <int W, int P>
 __device__ __forceinline__ int item_unit(uint32_t item, uint32_t inmask, uint32_t t, uint32_t slot, uint32_t own_o,
-                                         uint32_t own_nb_o, uint32_t desc_o, uint32_t ubuf_o, uint32_t tab_o,
+                                         uint32_t own_nb_o, uint32_t desc_o, uint32_t ubuf_o, const UnitThr& thr,
                                          uint32_t c_second, uint32_t k0, uint32_t k1) {
   static_assert(P == 2 || P == 4, "positions per item");
   constexpr int NI = kGroup / P;
@@ -263,15 +269,23 @@ __device__ __forceinline__ int item_unit(uint32_t item, uint32_t inmask, uint32_
     for (int d = 0; d < W; ++d) k += nbv[i * W + d];
     kk[i] = k;
   }
+  // x = (1 - 2b)(W - 2k); for x > 0 its threshold is thr.t[(W - x) / 2]
+  int xs[P];
+  uint32_t ths[P];
 #pragma unroll
   for (int i = 0; i < P; ++i) {
     const uint32_t b = (own >> (8 * i)) & 1u;
-    const uint64_t e = lds_u64(tab_o + 8u * (b * (uint32_t)(W + 1) + kk[i]));
-    const uint32_t thr = (uint32_t)e;
-    const int x = (int)(uint32_t)(e >> 32);
+    const int v = W - 2 * (int)kk[i];
+    const int x = b ? -v : v;
+    const int jx = (W - x) >> 1;
+    uint32_t th32 = thr.t[0];
+    if constexpr (W > 2) th32 = jx == 1 ? thr.t[1] : th32;
+    if constexpr (W > 4) th32 = jx == 2 ? thr.t[2] : th32;
+    xs[i] = x;
+    ths[i] = th32;
     // position q = P j + i of the group: half q & 1 (= i & 1) of word q >> 1
     const uint32_t prim = (words[i >> 1] >> ((i & 1) * 16)) & 0xFFFFu;
-    const uint32_t th = thr >> 16;
+    const uint32_t th = th32 >> 16;
     const bool in = (inmask >> i) & 1u;
     const bool acc = in & ((x <= 0) | (prim < th));
     flips |= (uint32_t)acc << i;
@@ -282,12 +296,10 @@ __device__ __forceinline__ int item_unit(uint32_t item, uint32_t inmask, uint32_
 #pragma unroll
     for (int i = 0; i < P; ++i)
       if ((ties >> i) & 1u) {
-        const uint32_t b = (own >> (8 * i)) & 1u;
-        const uint64_t e = lds_u64(tab_o + 8u * (b * (uint32_t)(W + 1) + kk[i]));
         const U4 r2 = philox(U4{(uint32_t)(p0 + i), t, slot, c_second}, k0, k1);
-        if ((r2.x & 0xFFFFu) < ((uint32_t)e & 0xFFFFu)) {
+        if ((r2.x & 0xFFFFu) < (ths[i] & 0xFFFFu)) {
           flips |= 1u << i;
-          dacc += 2 * (int)(uint32_t)(e >> 32);
+          dacc += 2 * xs[i];
         }
       }
   }
