@@ -167,7 +167,7 @@ namespace {
 struct LaunchPlan {
   int rpc, threads, in_smem, grid, p;
   int cluster;  // > 0: the grid is one cluster of this many CTAs
-  int unit;     // 1: the unit-regular item form
+  int unit;     // > 0: the unit-regular item form, compiled for this many colour phases at most
   size_t smem;
 };
 
@@ -285,6 +285,7 @@ int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPl
     // items of the largest colour class: a class of m positions touches at most (m + 14) / 8 groups
     auto items_of = [&](int P_) { return ((p->max_class + 14) / kGroup) * (kGroup / P_); };
     const int PU = P_user ? P_user : unit_auto_positions(p->max_class);
+    const int uph = p->n_colors <= 2 ? 2 : kUnitPhases;  // the instance compiled for these phases
     auto total_u = [&](int threads_, bool cl) {
       return smem_layout(p->n_pos, 1, R, p->max_field, p->n_colors, p->n_slices, p->n_ell, true, true, threads_, cl,
                          W, PU)
@@ -294,7 +295,7 @@ int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPl
     const int threads = r->threads_per_cta > 0 ? r->threads_per_cta : ((items_of(PU) + 31) / 32) * 32;
     if (threads >= items_of(PU) && threads <= unit_max_threads(PU) && threads % 32 == 0) {
       if (mode != 1 && R >= 2 && R <= kMaxCluster && total_u(threads, true) <= (size_t)di.max_smem_optin) {
-        const void* fn = run_kernel_ptr(ip, 1, W, W, 0, PU, 1, 1);
+        const void* fn = run_kernel_ptr(ip, 1, W, W, 0, PU, 1, uph);
         const size_t smem = total_u(threads, true);
         int per_sm = 0;
         bool ok = false;
@@ -303,12 +304,12 @@ int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPl
         rc = cluster_fits(fn, R, threads, smem, &ok);
         if (rc) return rc;
         if (ok) {
-          *lp = LaunchPlan{1, threads, 1, R, PU, R, 1, smem};
+          *lp = LaunchPlan{1, threads, 1, R, PU, R, uph, smem};
           return DRIFT_PT_OK;
         }
       }
       if (mode != 2 && total_u(threads, false) <= (size_t)di.max_smem_optin) {
-        const void* fn = run_kernel_ptr(ip, 1, W, W, 0, PU, 0, 1);
+        const void* fn = run_kernel_ptr(ip, 1, W, W, 0, PU, 0, uph);
         const size_t smem = total_u(threads, false);
         int per_sm = 0;
         rc = prepare_kernel(fn, threads, smem, &per_sm);
@@ -316,7 +317,7 @@ int plan_launch(const DriftPtDeviceProblem* p, const DriftPtRunArgs* r, LaunchPl
         if ((long long)per_sm * di.sm_count >= R) {
           // Chosen over every form of the gather: on B200 it ran 2-D EA L = 16 with 24 replicas and a
           // swap after every sweep at 3.4 attempts/ns against 2.6 for the gather's cluster form.
-          *lp = LaunchPlan{1, threads, 1, R, PU, 0, 1, smem};
+          *lp = LaunchPlan{1, threads, 1, R, PU, 0, uph, smem};
           return DRIFT_PT_OK;
         }
       }

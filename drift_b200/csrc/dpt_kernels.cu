@@ -113,7 +113,11 @@ __device__ __forceinline__ int ld_relaxed_i32(const int* p) {
 // 16-bit neighbour addresses from a table staged at launch instead of gathering the sliced ELL,
 // spins live as 0/1 bytes with a flipped copy, and each group's Philox block is computed once per
 // sweep, a sweep ahead, into shared memory (item_unit).
-template <bool kInt, bool kInSmem, int W, bool kExactW, bool kField, int P, bool kCluster, int kUnitW = 0>
+// kPh: the unit-regular form's most colour phases (2 for bipartite problems, else kUnitPhases), so
+// that a thread's per-phase state (item, Philox duty, neighbour-address row) takes no registers for
+// phases the problem does not have.
+template <bool kInt, bool kInSmem, int W, bool kExactW, bool kField, int P, bool kCluster, int kUnitW = 0,
+          int kPh = kUnitPhases>
 __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads, 1) pt_run_kernel(const PtKernelArgs a) {
   constexpr bool kUnit = kUnitW > 0;
   static_assert(kUnit || P == 8 || (kInt && (P == 4 || P == 1)), "positions per item");
@@ -310,11 +314,16 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
   // issue-bound, while in the large phases the blocks overlap other warps' items. Spreading them
   // over every phase's threads without an item, so that no thread runs both, measured +0.2 %.) The
   // host makes the CTA wide enough for one item per thread and phase.
-  uint32_t s_item[kUnitPhases], s_px[kUnitPhases];
+  // Rows of neighbour addresses of at most 16 bytes are kept in registers too (s_row).
+  constexpr bool kRowReg = kUnit && unit_row_in_registers<kUnitW, P>();
+  constexpr int kRB = ((2 * P * kUnitW + 7) / 8) * 8;
+  uint32_t s_item[kPh], s_px[kPh];
+  uint4 s_row[kPh];
 #pragma unroll
-  for (int c = 0; c < kUnitPhases; ++c) {
+  for (int c = 0; c < kPh; ++c) {
     s_item[c] = 0u;
     s_px[c] = 0u;
+    s_row[c] = make_uint4(0u, 0u, 0u, 0u);
     if (kUnit && c < k) {
       const int lo = cptr[c], hi = cptr[c + 1];
       const int glo = lo >> 3, ghi = (hi + 7) >> 3;
@@ -323,6 +332,15 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
         const uint32_t msk = range_mask<P>((int)item * P, lo, hi);
         const uint32_t word = reinterpret_cast<const uint16_t*>(smem + L.h)[(item * P) >> 2];
         s_item[c] = msk ? (item | (msk << 14) | (word << 18) | 0x80000000u) : 0u;
+        if constexpr (kRowReg) {
+          const uint32_t row = (uint32_t)L.nbr + item * (uint32_t)kRB;
+          if constexpr (kRB == 16) {
+            s_row[c] = lds_u128(row);
+          } else {
+            const uint64_t v = lds_u64(row);
+            s_row[c] = make_uint4((uint32_t)v, (uint32_t)(v >> 32), 0u, 0u);
+          }
+        }
       }
       const int gp = (lo + 7) / kGroup + (tps - 1 - lt);
       if (gp < (hi + 7) / kGroup) s_px[c] = (uint32_t)gp + 1u;
@@ -485,15 +503,15 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
         const uint32_t ng = (uint32_t)(n_pos / kGroup);
         const uint32_t ubuf = (uint32_t)L.w + 16u * ng * (t & 1u), unext = (uint32_t)L.w + 16u * ng * ((t + 1u) & 1u);
 #pragma unroll
-        for (int c = 0; c < kUnitPhases; ++c) {
+        for (int c = 0; c < kPh; ++c) {
           if (c < k) {
             if (s_px[c]) unit_next_block(s_px[c] - 1u, t, (uint32_t)my_slot, unext, c_sweep, a.k0, a.k1);
             if (s_item[c] >> 31) {
               const uint32_t item = s_item[c] & 0x3FFFu;
               const uint32_t own_o = my_sp_o + 4u * ((s_item[c] >> 18) & 0x1FFFu) + ((item * P) & 3u);
               dacc_u += item_unit<kUnitW, P>(item, (s_item[c] >> 14) & 0xFu, t, (uint32_t)my_slot, own_o,
-                                           own_o + (uint32_t)n_pos, (uint32_t)L.nbr, ubuf, uthr, c_second, a.k0,
-                                           a.k1);
+                                           own_o + (uint32_t)n_pos, (uint32_t)L.nbr, s_row[c], ubuf, uthr,
+                                           c_second, a.k0, a.k1);
             }
             __syncthreads();
           }
@@ -918,15 +936,20 @@ static const void* pick_p(int max_w, int min_w, int p) {
   return pick_w<kInt, kInSmem, kField, 8, kCl>(max_w, min_w);
 }
 
-template <bool kCl, int P>
+template <bool kCl, int P, int kPh>
 static const void* pick_unit(int w) {
   switch (w) {
-    case 2: return (const void*)pt_run_kernel<true, true, 2, true, false, P, kCl, 2>;
-    case 3: return (const void*)pt_run_kernel<true, true, 3, true, false, P, kCl, 3>;
-    case 4: return (const void*)pt_run_kernel<true, true, 4, true, false, P, kCl, 4>;
-    case 6: return (const void*)pt_run_kernel<true, true, 6, true, false, P, kCl, 6>;
+    case 2: return (const void*)pt_run_kernel<true, true, 2, true, false, P, kCl, 2, kPh>;
+    case 3: return (const void*)pt_run_kernel<true, true, 3, true, false, P, kCl, 3, kPh>;
+    case 4: return (const void*)pt_run_kernel<true, true, 4, true, false, P, kCl, 4, kPh>;
+    case 6: return (const void*)pt_run_kernel<true, true, 6, true, false, P, kCl, 6, kPh>;
     default: return nullptr;
   }
+}
+
+template <bool kCl, int P>
+static const void* pick_unit_phases(int w, int phases) {
+  return phases <= 2 ? pick_unit<kCl, P, 2>(w) : pick_unit<kCl, P, kUnitPhases>(w);
 }
 
 bool unit_width_supported(int w) { return w == 2 || w == 3 || w == 4 || w == 6; }
@@ -937,8 +960,10 @@ const void* run_kernel_ptr(int integer_path, int in_smem, int max_width, int min
                            int positions_per_item, int cluster, int unit) {
   if (unit) {
     if (!integer_path || has_field || max_width != min_width) return nullptr;
-    if (positions_per_item == 2) return cluster ? pick_unit<true, 2>(max_width) : pick_unit<false, 2>(max_width);
-    if (positions_per_item == 4) return cluster ? pick_unit<true, 4>(max_width) : pick_unit<false, 4>(max_width);
+    if (positions_per_item == 2)
+      return cluster ? pick_unit_phases<true, 2>(max_width, unit) : pick_unit_phases<false, 2>(max_width, unit);
+    if (positions_per_item == 4)
+      return cluster ? pick_unit_phases<true, 4>(max_width, unit) : pick_unit_phases<false, 4>(max_width, unit);
     return nullptr;
   }
   const int p = positions_per_item, w = max_width, m = min_width;

@@ -112,7 +112,8 @@ __host__ __device__ inline SmemLayout smem_layout(int n_pos, int rpc, int R, int
 cudaError_t launch_init(const PtKernelArgs& a, int integer_path, cudaStream_t st);
 cudaError_t launch_energy_fp64(const PtKernelArgs& a, int integer_path, const int8_t* spins, int R, double* out,
                                cudaStream_t st);
-// unit > 0: the unit-regular form with positions_per_item = 2 or 4
+// unit > 0: the unit-regular form with positions_per_item = 2 or 4, compiled for `unit` colour phases
+// at most (2 or kUnitPhases; any value up to 2 picks the 2-phase instance)
 const void* run_kernel_ptr(int integer_path, int in_smem, int max_width, int min_width, int has_field,
                            int positions_per_item, int cluster = 0, int unit = 0);
 // widths the unit-regular form is compiled for
