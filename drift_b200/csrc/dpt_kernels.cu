@@ -499,7 +499,9 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
     for (int sw = 0; sw < a.spr; ++sw) {
       const uint32_t t = (uint32_t)(round * a.spr + sw);
       if constexpr (kUnit) {
-        // the static schedule: at most one item and one next-sweep Philox block per thread and phase
+        // the static schedule: at most one item and one next-sweep Philox block per thread and phase.
+        // The phase loop stays unrolled: a rolled loop (each phase's state picked by selects) ran
+        // MaxCut N = 4096 at 79 against 112 attempts/ns.
         const uint32_t ng = (uint32_t)(n_pos / kGroup);
         const uint32_t ubuf = (uint32_t)L.w + 16u * ng * (t & 1u), unext = (uint32_t)L.w + 16u * ng * ((t + 1u) & 1u);
 #pragma unroll
