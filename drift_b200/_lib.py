@@ -19,7 +19,7 @@ EXPORTED = (
     "drift_pt_version", "drift_pt_last_error", "drift_pt_greedy_coloring", "drift_pt_color_order",
     "drift_pt_layout_query", "drift_pt_layout_fill", "drift_pt_unit_placement", "drift_pt_thresholds",
     "drift_pt_workspace_bytes",
-    "drift_pt_init", "drift_pt_run", "drift_pt_check", "drift_pt_energy_fp64", "drift_pt_solve",
+    "drift_pt_init", "drift_pt_run", "drift_pt_check", "drift_pt_energy_fp64", "drift_pt_solve", "drift_pt_solve_release",
     "drift_pt_run_noalloc", "drift_pt_noalloc_check", "drift_pt_batch_items", "drift_pt_batch_init", "drift_pt_batch_workspace_bytes",
     "drift_pt_batch_run", "drift_pt_ms_workspace_bytes", "drift_pt_ms_init", "drift_pt_ms_run",
     "drift_pt_sk_quantize", "drift_pt_sk_layout_bytes", "drift_pt_sk_layout_fill", "drift_pt_sk_scales",

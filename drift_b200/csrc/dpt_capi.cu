@@ -543,12 +543,56 @@ extern "C" int drift_pt_energy_fp64(const DriftPtDeviceProblem* prob, const int8
 // ---------------------------------------------------------------------------------------------
 namespace {
 
-struct DeviceArena {
+// The device arena of drift_pt_solve, kept per thread and device across calls and grown when a call
+// needs more: a solve then allocates and frees no device memory when an earlier one on the same
+// thread was as large, and makes fewer driver calls (each a chance to wait on the driver's lock
+// while another process queries the GPU). Every array a solve reads is written by it first
+// (upload, initialisation), so nothing carries over from one call to the next.
+// drift_pt_solve_release frees it.
+struct SolveArena {
+  int dev = -1;
   void* base = nullptr;
-  ~DeviceArena() {
+  size_t cap = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  void release() {
     if (base) cudaFree(base);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    base = nullptr;
+    ev0 = ev1 = nullptr;
+    cap = 0;
+    dev = -1;
   }
+  ~SolveArena() { release(); }
 };
+
+SolveArena& thread_arena() {
+  static thread_local SolveArena a;
+  return a;
+}
+
+int solve_arena(size_t bytes, SolveArena** out) {
+  SolveArena& a = thread_arena();
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return set_error(DRIFT_PT_ECUDA, "cudaGetDevice failed");
+  if (a.dev != dev) a.release();
+  if (a.cap < bytes) {
+    if (a.base) cudaFree(a.base);
+    a.base = nullptr;
+    a.cap = 0;
+    const cudaError_t e = cudaMalloc(&a.base, bytes);
+    if (e != cudaSuccess) {
+      a.base = nullptr;
+      return set_error(DRIFT_PT_ENOMEM, "cudaMalloc of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    }
+    a.cap = bytes;
+  }
+  if (!a.ev0 && (cudaEventCreate(&a.ev0) != cudaSuccess || cudaEventCreate(&a.ev1) != cudaSuccess))
+    return set_error(DRIFT_PT_ECUDA, "solve: cudaEventCreate failed");
+  a.dev = dev;
+  *out = &a;
+  return DRIFT_PT_OK;
+}
 
 size_t bump(size_t& off, size_t bytes) {
   size_t o = off;
@@ -557,6 +601,12 @@ size_t bump(size_t& off, size_t bytes) {
 }
 
 }  // namespace
+
+extern "C" int drift_pt_solve_release(void) {
+  clear_error();
+  thread_arena().release();
+  return DRIFT_PT_OK;
+}
 
 extern "C" int drift_pt_solve(const DriftPtCsr* csr, const DriftPtSolveArgs* args, DriftPtSolveResult* out) {
   clear_error();
@@ -602,35 +652,41 @@ extern "C" int drift_pt_solve(const DriftPtCsr* csr, const DriftPtSolveArgs* arg
     rc = drift_pt_unit_placement(csr, 0, place.data());
     if (rc) return rc;
   }
-  // ---- device arena ----
+  // ---- device arena: the inputs first (one upload), then the results read back together, then
+  // the device-only state; the arena is kept per thread and device across calls ----
   size_t ws_bytes = 0;
   drift_pt_workspace_bytes(R, &ws_bytes);
   size_t off = 0;
   const size_t o_cp = bump(off, color_ptr.size() * 4), o_so = bump(off, slice_off.size() * 4),
                o_nb = bump(off, ell_nbr.size() * 4), o_w = bump(off, ell_w.size()), o_h = bump(off, h_pos.size()),
-               o_beta = bump(off, (size_t)R * 8), o_thr = bump(off, thr.size() * 4),
-               o_sp = bump(off, (size_t)R * info.n_pos), o_bsp = bump(off, (size_t)R * info.n_pos),
-               o_e = bump(off, (size_t)R * 8), o_be = bump(off, (size_t)R * 8), o_rs = bump(off, (size_t)R * 4),
-               o_sr = bump(off, (size_t)R * 4), o_tr = bump(off, (size_t)R * 8), o_ac = bump(off, (size_t)R * 8),
-               o_bh = bump(off, (size_t)std::max(1, args->n_rounds) * 8), o_ws = bump(off, ws_bytes),
-               o_pl = bump(off, place.size() * 2);
-  DeviceArena arena;
-  cudaError_t e = cudaMalloc(&arena.base, off);
-  if (e != cudaSuccess) {
-    arena.base = nullptr;
-    return set_error(DRIFT_PT_ENOMEM, "cudaMalloc of %zu bytes failed: %s", off, cudaGetErrorString(e));
+               o_beta = bump(off, (size_t)R * 8), o_thr = bump(off, thr.size() * 4), o_pl = bump(off, place.size() * 2);
+  const size_t up_bytes = off;
+  const size_t o_be = bump(off, (size_t)R * 8), o_e = bump(off, (size_t)R * 8), o_sr = bump(off, (size_t)R * 4),
+               o_tr = bump(off, (size_t)R * 8), o_ac = bump(off, (size_t)R * 8);
+  const size_t res_bytes = off - o_be;
+  const size_t o_bh = bump(off, (size_t)std::max(1, args->n_rounds) * 8), o_sp = bump(off, (size_t)R * info.n_pos),
+               o_bsp = bump(off, (size_t)R * info.n_pos), o_rs = bump(off, (size_t)R * 4), o_ws = bump(off, ws_bytes);
+  SolveArena* arena = nullptr;
+  rc = solve_arena(off, &arena);
+  if (rc) return rc;
+  unsigned char* d = static_cast<unsigned char*>(arena->base);
+  cudaError_t e;
+  {
+    std::vector<unsigned char> stage(up_bytes);
+    auto put = [&](size_t o, const void* src, size_t bytes) {
+      if (bytes) std::memcpy(stage.data() + o, src, bytes);
+    };
+    put(o_cp, color_ptr.data(), color_ptr.size() * 4);
+    put(o_so, slice_off.data(), slice_off.size() * 4);
+    put(o_nb, ell_nbr.data(), ell_nbr.size() * 4);
+    put(o_w, ell_w.data(), ell_w.size());
+    put(o_h, h_pos.data(), h_pos.size());
+    put(o_beta, betas.data(), (size_t)R * 8);
+    put(o_thr, thr.data(), thr.size() * 4);
+    put(o_pl, place.data(), place.size() * 2);
+    if ((e = cudaMemcpy(d, stage.data(), up_bytes, cudaMemcpyHostToDevice)) != cudaSuccess)
+      return cuda_fail(e, "solve: upload");
   }
-  unsigned char* d = static_cast<unsigned char*>(arena.base);
-  auto h2d = [&](size_t o, const void* src, size_t bytes) -> cudaError_t {
-    return bytes ? cudaMemcpy(d + o, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
-  };
-  if ((e = h2d(o_cp, color_ptr.data(), color_ptr.size() * 4)) != cudaSuccess ||
-      (e = h2d(o_so, slice_off.data(), slice_off.size() * 4)) != cudaSuccess ||
-      (e = h2d(o_nb, ell_nbr.data(), ell_nbr.size() * 4)) != cudaSuccess ||
-      (e = h2d(o_w, ell_w.data(), ell_w.size())) != cudaSuccess || (e = h2d(o_h, h_pos.data(), h_pos.size())) != cudaSuccess ||
-      (e = h2d(o_beta, betas.data(), (size_t)R * 8)) != cudaSuccess || (e = h2d(o_thr, thr.data(), thr.size() * 4)) != cudaSuccess ||
-      (e = h2d(o_pl, place.data(), place.size() * 2)) != cudaSuccess)
-    return cuda_fail(e, "solve: upload");
   DriftPtDeviceProblem prob;
   std::memset(&prob, 0, sizeof prob);
   prob.n = info.n;
@@ -671,29 +727,22 @@ extern "C" int drift_pt_solve(const DriftPtCsr* csr, const DriftPtSolveArgs* arg
   ra.thresholds = ip ? reinterpret_cast<const uint32_t*>(d + o_thr) : nullptr;
   rc = drift_pt_init(&prob, &ra, &st, nullptr);
   if (rc) return rc;
-  cudaEvent_t ev0, ev1;
-  cudaEventCreate(&ev0);
-  cudaEventCreate(&ev1);
-  cudaEventRecord(ev0, nullptr);
+  cudaEventRecord(arena->ev0, nullptr);
   rc = drift_pt_run(&prob, &ra, &st, d + o_ws, ws_bytes, nullptr);
-  cudaEventRecord(ev1, nullptr);
+  cudaEventRecord(arena->ev1, nullptr);
   if (rc == DRIFT_PT_OK) rc = drift_pt_check(d + o_ws, nullptr);
   float ms = 0.0f;
-  cudaEventElapsedTime(&ms, ev0, ev1);
-  cudaEventDestroy(ev0);
-  cudaEventDestroy(ev1);
+  cudaEventElapsedTime(&ms, arena->ev0, arena->ev1);
   if (rc) return rc;
-  // ---- results ----
-  std::vector<long long> be(R), en(R);
-  std::vector<int32_t> slot_of_rung(R);
-  std::vector<long long> tried(std::max(1, R - 1)), acc(std::max(1, R - 1));
-  if ((e = cudaMemcpy(be.data(), d + o_be, (size_t)R * 8, cudaMemcpyDeviceToHost)) != cudaSuccess ||
-      (e = cudaMemcpy(en.data(), d + o_e, (size_t)R * 8, cudaMemcpyDeviceToHost)) != cudaSuccess ||
-      (e = cudaMemcpy(slot_of_rung.data(), d + o_sr, (size_t)R * 4, cudaMemcpyDeviceToHost)) != cudaSuccess)
+  // ---- results: energies, bests, permutation and swap counts in one copy ----
+  std::vector<unsigned char> res(res_bytes);
+  if ((e = cudaMemcpy(res.data(), d + o_be, res_bytes, cudaMemcpyDeviceToHost)) != cudaSuccess)
     return cuda_fail(e, "solve: download");
-  if (R > 1 && ((e = cudaMemcpy(tried.data(), d + o_tr, (size_t)(R - 1) * 8, cudaMemcpyDeviceToHost)) != cudaSuccess ||
-                (e = cudaMemcpy(acc.data(), d + o_ac, (size_t)(R - 1) * 8, cudaMemcpyDeviceToHost)) != cudaSuccess))
-    return cuda_fail(e, "solve: download stats");
+  const long long* be = reinterpret_cast<const long long*>(res.data());
+  const long long* en = reinterpret_cast<const long long*>(res.data() + (o_e - o_be));
+  const int32_t* slot_of_rung = reinterpret_cast<const int32_t*>(res.data() + (o_sr - o_be));
+  const long long* tried = reinterpret_cast<const long long*>(res.data() + (o_tr - o_be));
+  const long long* acc = reinterpret_cast<const long long*>(res.data() + (o_ac - o_be));
   int best = 0;
   for (int r = 1; r < R; ++r)
     if (be[r] < be[best]) best = r;

@@ -707,6 +707,11 @@ typedef struct DriftPtSolveResult { /* caller-allocated host buffers; optional o
 
 DRIFT_PT_API int drift_pt_solve(const DriftPtCsr* csr, const DriftPtSolveArgs* args, DriftPtSolveResult* out);
 
+/* Frees the device arena drift_pt_solve keeps on the calling thread between calls (it is grown as
+ * calls need and otherwise freed when the thread exits). No counterpart in the reference, whose
+ * subprocess boundary frees everything with the process. */
+DRIFT_PT_API int drift_pt_solve_release(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -414,3 +414,34 @@ def test_solve_abi_matches_device_layer():
     assert np.array_equal(best_s, st["best_spins"][b].astype(np.float32))
     assert res.best_E == pytest.approx(model.energy(best_s.astype(np.float64)))
     assert res.throughput > 0 and 0.0 < res.swap_rate < 1.0
+
+
+def test_solve_calls_share_nothing_through_the_cached_arena():
+    """drift_pt_solve keeps its device arena on the thread between calls: a call after a larger and a
+    smaller one, and after drift_pt_solve_release, returns exactly what the same call returned first
+    (every output, the swap counts and the best-energy history included)."""
+    L = _lib.load()
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+
+    def solve(model, R, rounds, spr, seed):
+        hp = HostProblem.from_model(model)
+        betas = geometric_betas(R, 0.25, 5.0)
+        out = {"best_s": np.zeros(hp.n, np.float32), "rung_spins": np.zeros((R, hp.n), np.int8),
+               "rung_e": np.zeros(R), "tried": np.zeros(R - 1, np.int64), "acc": np.zeros(R - 1, np.int64),
+               "hist": np.zeros(rounds)}
+        args = _lib.SolveArgs(R, rounds, spr, 0, seed, 0.0, 0.0, p(betas))
+        res = _lib.SolveResult(0, 0, 0, 0, p(out["best_s"]), p(out["rung_spins"]), p(out["rung_e"]),
+                               p(out["tried"]), p(out["acc"]), p(out["hist"]))
+        _lib.check(L.drift_pt_solve(C.byref(hp.c_csr()), C.byref(args), C.byref(res)), "drift_pt_solve")
+        out["best_E"], out["swap_rate"] = res.best_E, res.swap_rate
+        return out
+
+    small = (maxcut_3regular(512, 3), 16, 12, 2, 5)
+    first = solve(*small)
+    solve(maxcut_3regular(2048, 6), 48, 30, 3, 9)  # a larger call grows the arena
+    again = solve(*small)
+    _lib.check(L.drift_pt_solve_release(), "drift_pt_solve_release")
+    fresh = solve(*small)
+    for k in first:
+        assert np.array_equal(first[k], again[k]), k
+        assert np.array_equal(first[k], fresh[k]), k
