@@ -541,7 +541,7 @@ def bench_b200(args):
         dist.destroy_process_group()
 
 
-# The other BASELINE workloads measured alongside the default line: (key, workload, overrides).
+# The other benchmark workloads measured alongside the default line: (key, workload, overrides).
 SECONDARIES = [
     ("ea2d_C1", "ea2d", {}),
     ("batched_er_C3", "batched_er", {}),
