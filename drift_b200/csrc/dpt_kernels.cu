@@ -554,6 +554,8 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
       // One slot per CTA. Each warp adds its threads' energy changes as two 32-bit sums, of the low
       // 16 bits and of the rest, so no sum can overflow; after one barrier every thread adds the
       // warps' sums itself and holds the slot's new energy. Integer sums: any order, the same bits.
+      // (Storing the warps' sums before the last colour phase's barrier instead, to save this
+      // barrier, measured slower: MaxCut N = 4096 111.6 -> 107.8, 2-D EA L = 16 3.88 -> 3.60.)
       const int lane = tid & 31, wid = tid >> 5;
       double u_first = 0.0;
       if (!unit_helper && tid < 32) u_first = swap_uniform(round, tid);
