@@ -400,10 +400,11 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
     return abort_now ? 0ll : __ldcg(a.pub + at);
   };
   // The decision of pair (r, r + 1) of round `round` between slots sa (rung r) and sb (rung r + 1)
-  // with energy difference de = E(sa) - E(sb); u_first is the uniform of the lane's first pair.
-  auto decide_pair = [&](long long round, int r, int sa, int sb, long long de, double u_first) {
+  // with energy difference de = E(sa) - E(sb) and dbeta = beta_r - beta_{r+1}; u_first is the
+  // uniform of the lane's first pair.
+  auto decide_pair = [&](long long round, int r, int sa, int sb, long long de, double dbeta, double u_first) {
     const double ded = kInt ? (double)de : d_mul((double)de, kFloatEnergyScale);
-    const double delta = d_mul(d_sub(beta_sm[r], beta_sm[r + 1]), ded);
+    const double delta = d_mul(dbeta, ded);
     bool acc = delta >= 0.0;
     if (!acc) {
       double u = u_first;  // the first pair of the lane (r < 64)
@@ -430,7 +431,7 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
   auto exchange_lane = [&](long long round, double u_first, auto&& energy) {
     for (int r = (int)(round & 1) + 2 * tid; r + 1 < R; r += 64) {
       const int sa = slot_sm[r], sb = slot_sm[r + 1];
-      decide_pair(round, r, sa, sb, energy(sa) - energy(sb), u_first);
+      decide_pair(round, r, sa, sb, energy(sa) - energy(sb), d_sub(beta_sm[r], beta_sm[r + 1]), u_first);
     }
   };
   // Grid form: the energies of slots sa and sb (none when sb < 0) of round `round`, both polled at
@@ -611,6 +612,8 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
             const int r = (int)(round & 1) + 2 * lane;
             const bool has = r + 1 < R;
             const int sa = has ? slot_sm[r] : 0, sb = has ? slot_sm[r + 1] : 0;
+            // read before polling: the polls' memory clobbers keep the compiler from moving it later
+            const double dbeta = has ? d_sub(beta_sm[r], beta_sm[r + 1]) : 0.0;
             int abort_now = 0;
             long long e0 = 0, e1 = 0;
             poll_pair(round, lane < R ? lane : 0, lane + 32 < R ? lane + 32 : -1, e0, e1, abort_now);
@@ -620,7 +623,7 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
             } else {
               const long long a0 = __shfl_sync(0xffffffffu, e0, sa & 31), a1 = __shfl_sync(0xffffffffu, e1, sa & 31);
               const long long b0 = __shfl_sync(0xffffffffu, e0, sb & 31), b1 = __shfl_sync(0xffffffffu, e1, sb & 31);
-              if (has) decide_pair(round, r, sa, sb, (sa < 32 ? a0 : a1) - (sb < 32 ? b0 : b1), u_first);
+              if (has) decide_pair(round, r, sa, sb, (sa < 32 ? a0 : a1) - (sb < 32 ? b0 : b1), dbeta, u_first);
             }
           } else if (wid == 1 && blockIdx.x == 0 && a.best_hist) {
             int abort_now = 0;

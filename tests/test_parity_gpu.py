@@ -211,6 +211,7 @@ UNIT_CASES = {
     "ea3d_L6_W6_R20": (lambda: ea_3d(6, 4), 20, (0.2, 5.0), 60, 2, 3, 1),
     "ea3d_L4_W6_R12_cluster": (lambda: ea_3d(4, 5), 12, (0.2, 5.0), 60, 2, 4, 2),
     "ring_300_W2_R10": (lambda: _ring_pm(300, 6), 10, (0.2, 5.0), 80, 2, 5, 0),
+    "ring_301_three_classes_R20": (lambda: _ring_pm(301, 7), 20, (0.2, 5.0), 60, 3, 11, 1),
     "maxcut_3reg_4096_R64_C2": (lambda: maxcut_3regular(4096, 2), 64, (0.25, 5.0), 25, 4, 7, 0),
     "maxcut_3reg_2048_R16_cluster": (lambda: maxcut_3regular(2048, 5), 16, (0.25, 5.0), 20, 2, 5, 2),
     "one_replica": (lambda: maxcut_3regular(512, 3), 1, (0.2, 5.0), 40, 2, 8, 0),
@@ -221,10 +222,10 @@ UNIT_CASES = {
 
 @pytest.mark.parametrize("name", list(UNIT_CASES))
 def test_unit_regular_form_matches_oracle_bit_exact(name):
-    """The unit-regular form (neighbour addresses and a (spin, count) decision table in shared
-    memory) runs the oracle's chain bit for bit: lattices in 2-D and 3-D, a ring, MaxCut on 3-regular
-    graphs, padding positions (25 spins in 256 positions), one and two replicas, grid and cluster
-    round ends."""
+    """The unit-regular form (neighbour addresses, the rung's thresholds, a static schedule; compiled
+    for 2 or 4 colour phases) runs the oracle's chain bit for bit: lattices in 2-D and 3-D, rings
+    with 2 and 3 colour classes, MaxCut on 3-regular graphs, padding positions (25 spins in 256
+    positions), one and two replicas, grid and cluster round ends."""
     make, R, (tmin, tmax), rounds, spr, seed, sync = UNIT_CASES[name]
     model = make()
     betas = geometric_betas(R, tmin, tmax)
