@@ -20,7 +20,8 @@ constexpr int unit_max_threads(int P) { return P == 2 ? 832 : 1024; }
 // The form's choice of positions per item for a largest colour class of `max_class` spins: 2 while
 // one item per thread fits the 2-position CTA (a class touches at most (max_class + 14) / 8 groups).
 constexpr int unit_auto_positions(int max_class) { return (max_class + 14) / kGroup * 4 <= 832 ? 2 : 4; }
-// Colour classes the unit-regular form schedules statically (one register pair per class).
+// Colour classes the unit-regular form schedules statically (per class, a thread's item, Philox
+// duty and row of neighbour addresses in registers).
 constexpr int kUnitPhases = 4;
 
 int set_error(int code, const char* fmt, ...);
