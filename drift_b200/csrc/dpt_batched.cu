@@ -99,14 +99,19 @@ __device__ bool batch_grid_sync(const BatchArgs& a, unsigned long long k, int* c
     __threadfence();
     atomicAdd(a.bar, 1ULL);
     const unsigned long long target = k * gridDim.x;
-    const unsigned long long t0 = b_timer();
     int abort_now = 0;
-    while (b_ld_acquire(a.bar) < target) {
-      if (b_ld_relaxed(a.err) != 0) { abort_now = 1; break; }
-      if (b_timer() - t0 > (unsigned long long)a.timeout_ns) {
-        atomicExch(a.err, DRIFT_PT_ETIMEOUT);
-        abort_now = 1;
-        break;
+    // the error flag and the clock are read after the first unsuccessful poll and then after every
+    // 8th only (read after every poll they lengthen each poll)
+    if (b_ld_acquire(a.bar) < target) {
+      const unsigned long long t0 = b_timer();
+      for (int it = 1; b_ld_acquire(a.bar) < target; ++it) {
+        if (it != 1 && it % 8 != 0) continue;
+        if (b_ld_relaxed(a.err) != 0) { abort_now = 1; break; }
+        if (b_timer() - t0 > (unsigned long long)a.timeout_ns) {
+          atomicExch(a.err, DRIFT_PT_ETIMEOUT);
+          abort_now = 1;
+          break;
+        }
       }
     }
     *ctl_abort = abort_now;
