@@ -277,6 +277,14 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
   // runs this round's exchange, so they are ready in shared memory (by round parity) when needed.
   double* usw = reinterpret_cast<double*>(smem + L.usw);
   const bool unit_helper = kUnit && B >= 96;
+  // Grid form with at most 64 slots (warp 0 polls the energies, warp 1 of CTA 0 keeps the history,
+  // warp 2 draws the next swap uniforms): when the warps from 3 on have a thread for every group,
+  // the Philox blocks of the next round's first sweep are computed by them while the round's
+  // energies travel, instead of inside the last sweep's colour phases.
+  // Compiled into the 4-phase instances only: in the 2-phase instance of 2-D EA L = 16 (24 replicas,
+  // 96 threads, so never taken) its mere presence cost 7 %, while on MaxCut N = 4096 it gained 4.5 %.
+  const bool unit_defer_px = kPh > 2 && unit_helper && !kCluster && gridDim.x > 1 && a.R <= 64 &&
+                             B - 96 >= (a.n + kGroup - 1) / kGroup;
   if (unit_helper && (tid >> 5) == 2) usw[tid & 31] = swap_uniform(a.round0, tid & 31);
   if (tid == 0) {
     ctl[0] = 0;  // abort flag
@@ -508,7 +516,8 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
 #pragma unroll
         for (int c = 0; c < kPh; ++c) {
           if (c < k) {
-            if (s_px[c]) unit_next_block(s_px[c] - 1u, t, (uint32_t)my_slot, unext, c_sweep, a.k0, a.k1);
+            if (s_px[c] && !(unit_defer_px && sw == a.spr - 1))
+              unit_next_block(s_px[c] - 1u, t, (uint32_t)my_slot, unext, c_sweep, a.k0, a.k1);
             if (s_item[c] >> 31) {
               const uint32_t item = s_item[c] & 0x3FFFu;
               const uint32_t own_o = my_sp_o + 4u * ((s_item[c] >> 18) & 0x1FFFu) + ((item * P) & 3u);
@@ -649,6 +658,13 @@ __global__ void __launch_bounds__(kUnitW > 0 ? unit_max_threads(P) : kMaxThreads
         }
       }
       if (unit_helper && wid == 2) usw[((j + 1) & 1) * 32 + lane] = swap_uniform(round + 1, lane);
+      if (unit_defer_px && tid >= 96 && tid - 96 < (a.n + kGroup - 1) / kGroup) {
+        // the next round's first sweep t + 1 = (round + 1) spr: its blocks, from this round's last sweep t
+        const uint32_t tl = (uint32_t)(round * a.spr + a.spr - 1);
+        const uint32_t ng = (uint32_t)(n_pos / kGroup);
+        unit_next_block((uint32_t)(tid - 96), tl, (uint32_t)my_slot,
+                        (uint32_t)L.w + 16u * ng * ((tl + 1u) & 1u), c_sweep, a.k0, a.k1);
+      }
       __syncthreads();
       if (ctl[0]) break;
     } else {
