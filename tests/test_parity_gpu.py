@@ -213,6 +213,9 @@ UNIT_CASES = {
     "ring_300_W2_R10": (lambda: _ring_pm(300, 6), 10, (0.2, 5.0), 80, 2, 5, 0),
     "ring_301_three_classes_R20": (lambda: _ring_pm(301, 7), 20, (0.2, 5.0), 60, 3, 11, 1),
     "maxcut_3reg_4096_R64_C2": (lambda: maxcut_3regular(4096, 2), 64, (0.25, 5.0), 25, 4, 7, 0),
+    # padding positions (1800 spins in 2048) with the next round's first-sweep Philox blocks computed
+    # in the round end (grid form, 352 threads: 256 beyond the first three warps for 225 groups)
+    "maxcut_3reg_1800_R40_padded_deferred": (lambda: maxcut_3regular(1800, 9), 40, (0.25, 5.0), 30, 3, 13, 1),
     "maxcut_3reg_2048_R16_cluster": (lambda: maxcut_3regular(2048, 5), 16, (0.25, 5.0), 20, 2, 5, 2),
     "one_replica": (lambda: maxcut_3regular(512, 3), 1, (0.2, 5.0), 40, 2, 8, 0),
     "two_replicas": (lambda: maxcut_3regular(512, 3), 2, (0.2, 5.0), 40, 2, 9, 0),
